@@ -1,0 +1,317 @@
+// flb_lattice.cuh -- D3Q19 constants, population storage forms and the
+// per-cell collision operators of the stream-and-collide path.
+//
+// Everything here is device code compiled for sm_100a.  The arithmetic of each
+// operator follows the reference policy it replaces (cited per function) so the
+// FP32 results stay within rounding of the reference's CPU path.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+
+namespace flb {
+
+constexpr int Q = 19;
+
+// D3Q19 velocities in the reference ordering (src/lbm/lattice_set.h:263-266):
+// rest, 6 axis directions, 12 diagonals; opposite of odd i is i+1.
+__host__ __device__ constexpr int cx(int i) {
+  constexpr int v[Q] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0};
+  return v[i];
+}
+__host__ __device__ constexpr int cy(int i) {
+  constexpr int v[Q] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1};
+  return v[i];
+}
+__host__ __device__ constexpr int cz(int i) {
+  constexpr int v[Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1};
+  return v[i];
+}
+__host__ __device__ constexpr int opp(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+
+// Weights as the reference evaluates its Fraction<> table: T(num)/T(den).
+template <typename R>
+__host__ __device__ constexpr R weight(int i) {
+  return i == 0 ? R(1) / R(3) : (i < 7 ? R(1) / R(18) : R(1) / R(36));
+}
+
+// ---------------------------------------------------------------------------
+// D3Q19 Gram-Schmidt moment basis (d'Humieres, Ginzburg, Krafczyk, Lallemand,
+// Luo, Phil. Trans. R. Soc. A 360 (2002)), rows in the paper's order
+// (rho, e, eps, jx, qx, jy, qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz,
+// mx, my, mz), evaluated on the reference velocity ordering.  The reference
+// provides the generic algorithm (src/lbm/collisionMRT.h:132-190) but no D3Q19
+// matrix.
+__host__ __device__ constexpr int mrt_m(int k, int i) {
+  const int x = cx(i), y = cy(i), z = cz(i);
+  const int c2 = x * x + y * y + z * z;
+  return k == 0    ? 1
+         : k == 1  ? 19 * c2 - 30
+         : k == 2  ? (21 * c2 * c2 - 53 * c2 + 24) / 2
+         : k == 3  ? x
+         : k == 4  ? (5 * c2 - 9) * x
+         : k == 5  ? y
+         : k == 6  ? (5 * c2 - 9) * y
+         : k == 7  ? z
+         : k == 8  ? (5 * c2 - 9) * z
+         : k == 9  ? 3 * x * x - c2
+         : k == 10 ? (3 * c2 - 5) * (3 * x * x - c2)
+         : k == 11 ? y * y - z * z
+         : k == 12 ? (3 * c2 - 5) * (y * y - z * z)
+         : k == 13 ? x * y
+         : k == 14 ? y * z
+         : k == 15 ? x * z
+         : k == 16 ? x * (y * y - z * z)
+         : k == 17 ? y * (z * z - x * x)
+                   : z * (x * x - y * y);
+}
+__host__ __device__ constexpr int mrt_norm(int k) {
+  int s = 0;
+  for (int i = 0; i < Q; ++i) s += mrt_m(k, i) * mrt_m(k, i);
+  return s;
+}
+// Moments that are even under c -> -c (depend on f_i + f_opp(i) only).
+__host__ __device__ constexpr bool mrt_even(int k) {
+  return k == 0 || k == 1 || k == 2 || (k >= 9 && k <= 15);
+}
+__host__ __device__ constexpr bool mrt_conserved(int k) {
+  return k == 0 || k == 3 || k == 5 || k == 7;
+}
+__host__ __device__ constexpr bool mrt_shear(int k) {
+  return k == 9 || k == 11 || k == 13 || k == 14 || k == 15;
+}
+
+// ---------------------------------------------------------------------------
+// Storage forms.  Load converts a stored population to the arithmetic type R,
+// store converts back.  FP16S keeps (f_i - rho0*w_i) * scale in binary16
+// (round to nearest even); scale is a power of two so the shift/scale are exact.
+template <typename S, typename R>
+struct Storage;
+
+template <>
+struct Storage<float, float> {
+  __device__ static __forceinline__ float load(const float* p, float, float) { return *p; }
+  __device__ static __forceinline__ void store(float* p, float v, float, float) { *p = v; }
+};
+
+template <>
+struct Storage<double, double> {
+  __device__ static __forceinline__ double load(const double* p, double, double) { return *p; }
+  __device__ static __forceinline__ void store(double* p, double v, double, double) { *p = v; }
+};
+
+template <>
+struct Storage<__half, float> {
+  __device__ static __forceinline__ float load(const __half* p, float shift, float inv_scale) {
+    return fmaf(__half2float(*p), inv_scale, shift);
+  }
+  __device__ static __forceinline__ void store(__half* p, float v, float shift, float scale) {
+    *p = __float2half_rn((v - shift) * scale);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Per-cell operators.  f[] holds the 19 populations of one cell in registers.
+
+// moment::rhoUImpl<D3Q19> (src/lbm/moment.ur.h:505-517)
+template <typename R>
+__device__ __forceinline__ void rho_u(const R* f, R& rho, R& ux, R& uy, R& uz) {
+  rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
+        f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+  ux = (f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16]) / rho;
+  uy = (f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18]) / rho;
+  uz = (f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18]) / rho;
+}
+
+// equilibrium::SecondOrderImpl<D3Q19> (src/lbm/equilibrium.ur.h:166-215)
+template <typename R>
+__device__ __forceinline__ void feq2(R* feq, R rho, R ux, R uy, R uz) {
+  const R InvCs2 = R(3);
+  const R var0 = R(1) - (ux * ux + uy * uy + uz * uz) * (R(0.5) * InvCs2);
+  const R rw0 = weight<R>(0) * rho;
+  const R rw1 = weight<R>(1) * rho;
+  const R rw7 = weight<R>(7) * rho;
+  const R k1 = InvCs2 * ux, v1 = var0 + k1 * k1 * R(0.5);
+  const R k3 = InvCs2 * uy, v3 = var0 + k3 * k3 * R(0.5);
+  const R k5 = InvCs2 * uz, v5 = var0 + k5 * k5 * R(0.5);
+  const R k7 = InvCs2 * (ux + uy), v7 = var0 + k7 * k7 * R(0.5);
+  const R k9 = InvCs2 * (ux + uz), v9 = var0 + k9 * k9 * R(0.5);
+  const R k11 = InvCs2 * (uy + uz), v11 = var0 + k11 * k11 * R(0.5);
+  const R k13 = InvCs2 * (ux - uy), v13 = var0 + k13 * k13 * R(0.5);
+  const R k15 = InvCs2 * (ux - uz), v15 = var0 + k15 * k15 * R(0.5);
+  const R k17 = InvCs2 * (uy - uz), v17 = var0 + k17 * k17 * R(0.5);
+  feq[0] = rw0 * var0;
+  feq[1] = rw1 * (v1 + k1);
+  feq[2] = rw1 * (v1 - k1);
+  feq[3] = rw1 * (v3 + k3);
+  feq[4] = rw1 * (v3 - k3);
+  feq[5] = rw1 * (v5 + k5);
+  feq[6] = rw1 * (v5 - k5);
+  feq[7] = rw7 * (v7 + k7);
+  feq[8] = rw7 * (v7 - k7);
+  feq[9] = rw7 * (v9 + k9);
+  feq[10] = rw7 * (v9 - k9);
+  feq[11] = rw7 * (v11 + k11);
+  feq[12] = rw7 * (v11 - k11);
+  feq[13] = rw7 * (v13 + k13);
+  feq[14] = rw7 * (v13 - k13);
+  feq[15] = rw7 * (v15 + k15);
+  feq[16] = rw7 * (v15 - k15);
+  feq[17] = rw7 * (v17 + k17);
+  feq[18] = rw7 * (v17 - k17);
+}
+
+// collision::BGK (src/lbm/collision.h:40-57): f <- omega*feq + (1-omega)*f
+template <typename R>
+__device__ __forceinline__ void bgk(R* f, R omega, R omega_c) {
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  feq2(feq, rho, ux, uy, uz);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = omega * feq[i] + omega_c * f[i];
+}
+
+// collision::BGK<moment::useFieldrhoU, ...>: rho, u from the fields.
+template <typename R>
+__device__ __forceinline__ void bgk_field(R* f, R omega, R omega_c, R rho, R ux, R uy, R uz) {
+  R feq[Q];
+  feq2(feq, rho, ux, uy, uz);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = omega * feq[i] + omega_c * f[i];
+}
+
+// collision::BounceBack<D3Q19> (src/lbm/collision.ur.h:62-93): swap i, i+1.
+template <typename R>
+__device__ __forceinline__ void bounce_back(R* f) {
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const R t = f[i];
+    f[i] = f[i + 1];
+    f[i + 1] = t;
+  }
+}
+
+// collision::BounceBackMovingWall<D3Q19> (src/lbm/collision.ur.h:130-187):
+// f_i <- f_opp + 6 w_i rho_w (u_w.c_i), f_opp <- f_i - same, i odd.
+template <typename R>
+__device__ __forceinline__ void moving_wall(R* f, R rho_w, R ux, R uy, R uz) {
+  const R rhox = R(6) * rho_w;
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    R uc;
+    const int a = cx(i), b = cy(i), c = cz(i);
+    // u.c_i evaluated in the reference's term order (u0 +/- u1 etc.)
+    if (b == 0 && c == 0) uc = ux;
+    else if (a == 0 && c == 0) uc = uy;
+    else if (a == 0 && b == 0) uc = uz;
+    else if (c == 0) uc = (b > 0) ? ux + uy : ux - uy;
+    else if (b == 0) uc = (c > 0) ? ux + uz : ux - uz;
+    else uc = (c > 0) ? uy + uz : uy - uz;
+    uc = uc * weight<R>(i) * rhox;
+    const R t = f[i];
+    f[i] = f[i + 1] + uc;
+    f[i + 1] = t - uc;
+  }
+}
+
+// collision::SmagorinskyBGK (src/lbm/collisionLES.h:36-62) with
+// moment::Pi_ab_neq<D3Q19> (src/lbm/moment.ur.h:751-762).  The momenta scheme
+// writes RHO, so the density in the eddy-viscosity coefficient is this cell's
+// current rho.  cs_coeff = Cs^2 * 9 * 2 * sqrt(2) is precomputed on the host in
+// double, as the reference evaluates that product in double.
+template <typename R>
+__device__ __forceinline__ void smagorinsky_bgk(R* f, R rt_mol, R cs_coeff) {
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  const R cs2 = R(1) / R(3);
+  const R p0 = f[1] + f[2] + f[7] + f[8] + f[9] + f[10] + f[13] + f[14] + f[15] + f[16] -
+               rho * (ux * ux + cs2);
+  const R p1 = f[7] + f[8] - f[13] - f[14] - rho * (ux * uy);
+  const R p2 = f[9] + f[10] - f[15] - f[16] - rho * (ux * uz);
+  const R p3 = f[3] + f[4] + f[7] + f[8] + f[11] + f[12] + f[13] + f[14] + f[17] + f[18] -
+               rho * (uy * uy + cs2);
+  const R p4 = f[11] + f[12] - f[17] - f[18] - rho * (uy * uz);
+  const R p5 = f[5] + f[6] + f[9] + f[10] + f[11] + f[12] + f[15] + f[16] + f[17] + f[18] -
+               rho * (uz * uz + cs2);
+  const R nsq = p0 * p0 + p1 * p1 * R(2) + p2 * p2 * R(2) + p3 * p3 + p4 * p4 * R(2) + p5 * p5;
+  const R norm = sqrt(nsq);
+  const R coeff = cs_coeff / rho;
+  const R rt_tur = R(0.5) * (sqrt(rt_mol * rt_mol + coeff * norm) - rt_mol);
+  const R eomega = R(1) / (rt_mol + rt_tur);
+  const R eomega_c = R(1) - eomega;
+  feq2(feq, rho, ux, uy, uz);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = eomega * feq[i] + eomega_c * f[i];
+}
+
+// collision::MRT_Feq_RhoU (src/lbm/collisionMRT.h:142-188):
+//   f <- f - M^-1 S (M f - M feq),  M^-1[i][k] = M[k][i] / |M_k|^2.
+// Evaluated on f - feq with the basis split into moments even and odd under
+// c -> -c, so even moments see only f_i + f_opp and odd ones only f_i - f_opp;
+// all basis entries are compile-time constants (zeros and unit factors fold).
+// s[k] already holds the per-moment rate divided by |M_k|^2.
+template <typename R>
+__device__ __forceinline__ void mrt(R* f, const R* s_over_norm) {
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  feq2(feq, rho, ux, uy, uz);
+  R a[9], b[9];  // symmetric / antisymmetric non-equilibrium parts per pair
+  const R r0 = f[0] - feq[0];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    const R n1 = f[2 * p + 1] - feq[2 * p + 1];
+    const R n2 = f[2 * p + 2] - feq[2 * p + 2];
+    a[p] = n1 + n2;
+    b[p] = n1 - n2;
+  }
+  R mu[Q];
+#pragma unroll
+  for (int k = 0; k < Q; ++k) {
+    if (mrt_conserved(k)) {
+      mu[k] = R(0);
+      continue;
+    }
+    R m = R(0);
+    if (mrt_even(k)) {
+      if (mrt_m(k, 0) != 0) m = R(mrt_m(k, 0)) * r0;
+#pragma unroll
+      for (int p = 0; p < 9; ++p) {
+        const int c = mrt_m(k, 2 * p + 1);
+        if (c == 1) m += a[p];
+        else if (c == -1) m -= a[p];
+        else if (c != 0) m += R(c) * a[p];
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < 9; ++p) {
+        const int c = mrt_m(k, 2 * p + 1);
+        if (c == 1) m += b[p];
+        else if (c == -1) m -= b[p];
+        else if (c != 0) m += R(c) * b[p];
+      }
+    }
+    mu[k] = m * s_over_norm[k];
+  }
+  // back-transform: delta f_i = sum_k M[k][i] mu_k
+  R d0 = R(0);
+#pragma unroll
+  for (int k = 0; k < Q; ++k)
+    if (mrt_even(k) && !mrt_conserved(k) && mrt_m(k, 0) != 0) d0 += R(mrt_m(k, 0)) * mu[k];
+  f[0] -= d0;
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    R e = R(0), o = R(0);
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      if (mrt_conserved(k)) continue;
+      const int c = mrt_m(k, 2 * p + 1);
+      if (c == 0) continue;
+      if (mrt_even(k)) e += R(c) * mu[k];
+      else o += R(c) * mu[k];
+    }
+    f[2 * p + 1] -= e + o;
+    f[2 * p + 2] -= e - o;
+  }
+}
+
+}  // namespace flb

@@ -1,0 +1,180 @@
+/* flb.h -- C ABI of the B200 D3Q19 stream-and-collide library (libflb_b200.so).
+ *
+ * This is the drop-in boundary for FreeLB's lattice-Boltzmann hot path.  The
+ * reference exposes that path only as C++ templates (no ABI); each entry point
+ * below names the reference member it replaces.  Host-side C++17 classes with
+ * the reference's names (freelb_b200/cpp/freelb.h) and the Python module
+ * freelb_b200 call through this header.
+ *
+ * Conventions (all entry points):
+ *   - return FLB_OK (0) or a negative FLB_ERR_* code; nothing calls exit();
+ *     flb_last_error() gives a message for the calling host thread.
+ *   - plain pointers and sizes only; `stream` is a cudaStream_t passed as
+ *     void* (NULL = legacy default stream).  Every device operation is
+ *     ordered on that stream.  Host buffers are owned by the caller; device
+ *     memory is owned by the handle.  Calls that read or write host memory
+ *     synchronise `stream` before returning.
+ *   - a handle is used from one host thread at a time.
+ *   - cell indexing is the reference's: id = x + nx*(y + ny*z) over the stored
+ *     mesh (interior + overlap layer), x fastest (BasicBlock::getIndex,
+ *     src/geometry/basic_geometry.h:310-330); populations are 19 arrays of N
+ *     cells in D3Q19 order (src/lbm/lattice_set.h:263-266), each array in the
+ *     logical (post-rotation) order of CyclicArray::operator[]
+ *     (src/data_struct/field.h:626-629).
+ */
+#ifndef FLB_H_
+#define FLB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLB_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FLB_API __attribute__((visibility("default")))
+#else
+#define FLB_API
+#endif
+
+/* status codes */
+#define FLB_OK 0
+#define FLB_ERR_INVALID (-1)     /* bad argument or descriptor */
+#define FLB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define FLB_ERR_OOM (-3)         /* device allocation failed */
+#define FLB_ERR_TIMEOUT (-4)     /* a bounded device wait gave up */
+#define FLB_ERR_NUMERIC (-5)     /* non-finite population detected */
+#define FLB_ERR_UNSUPPORTED (-6) /* combination not built */
+#define FLB_ERR_STATE (-7)       /* call not valid in the handle's state */
+
+/* population storage in HBM */
+#define FLB_STORAGE_FP32 0  /* f_i as float */
+#define FLB_STORAGE_FP16S 1 /* f_i - rho0*w_i as half, float arithmetic */
+#define FLB_STORAGE_FP64 2  /* f_i as double, double arithmetic */
+
+/* bulk collision model (the policy bound to FLB_OP_BULK) */
+#define FLB_MODEL_BGK 0 /* collision::BGK<moment::rhoU, equilibrium::SecondOrder> */
+#define FLB_MODEL_MRT 1 /* collision::MRT_Feq_RhoU, D3Q19 Gram-Schmidt basis */
+#define FLB_MODEL_LES 2 /* collision::SmagorinskyBGK<moment::rhoU<CELL,true>, ...> */
+
+/* per-flag operations (the policy of a tmp::Key_TypePair) */
+#define FLB_OP_NONE 0       /* no collision (void cells) */
+#define FLB_OP_BULK 1       /* the bulk model above */
+#define FLB_OP_BOUNCEBACK 2 /* collision::BounceBack (full-way swap) */
+#define FLB_OP_MOVINGWALL 3 /* collision::BounceBackMovingWall (RHO, VELOCITY fields) */
+#define FLB_OP_FIELD_BGK 4  /* collision::BGK<moment::useFieldrhoU, SecondOrder> */
+
+/* host buffer element types */
+#define FLB_DTYPE_F32 0
+#define FLB_DTYPE_F64 1
+
+/* fields */
+#define FLB_FIELD_RHO 0      /* RHO<T>: N values */
+#define FLB_FIELD_VELOCITY 1 /* VELOCITY<T,3>: N x 3 values, AoS like Vector<T,3> */
+
+#define FLB_MAX_TASKS 8
+
+/* One block lattice.  Replaces the template arguments and constructor inputs
+ * of BlockLatticeManager<T, D3Q19<T>, TypePack<RHO, VELOCITY, POP>>
+ * (src/data_struct/block_lattice.h:234-433) plus the NSTask selector
+ * (src/utils/tmp.h:283-309): tasks are tried in order and a cell takes the op
+ * of the first task whose key shares a bit with its flag. */
+typedef struct flb_lattice_desc {
+  int nx, ny, nz;         /* stored cells per axis (interior + overlap) */
+  int storage;            /* FLB_STORAGE_* */
+  int model;              /* FLB_MODEL_* for FLB_OP_BULK cells */
+  double omega;           /* 1/tau: BlockLattice::Omega (block_lattice.hh:27-35) */
+  double smagorinsky;     /* Cs: SMAGORINSKY<T> (collisionLES.h:45) */
+  double mrt_rates[19];   /* s_k in moment order; entries 9,11,13,14,15 use omega */
+  double rho0;            /* reference density (init value, FP16S shift) */
+  int ntasks;             /* number of (key, op) pairs, <= FLB_MAX_TASKS */
+  uint8_t task_keys[FLB_MAX_TASKS];
+  uint8_t task_ops[FLB_MAX_TASKS];
+} flb_lattice_desc;
+
+typedef struct flb_lattice flb_lattice;
+
+/* Library identification: ABI version and the sm arch the kernels target. */
+FLB_API int flb_version(int* abi_version, int* sm_arch);
+
+/* Message for the last failed call on this host thread (never NULL). */
+FLB_API const char* flb_last_error(void);
+
+/* Fill `d` with the lid-driven cavity defaults: D3Q19 BGK, FP32, tasks
+ * {2: bulk, 4: bounce-back, 8: moving wall} as in
+ * benchmarks/cavity3d/cavity3d.cpp:173-182, rho0 = 1, MRT rates 1.2. */
+FLB_API int flb_desc_default(flb_lattice_desc* d, int nx, int ny, int nz, double tau);
+
+/* Allocate a block lattice on the current device.  Replaces the
+ * BlockLatticeManager constructor (block_lattice.hh:651-681); populations are
+ * initialised to rho0*w_i, RHO to rho0, VELOCITY to 0, flags to 1 (void). */
+FLB_API int flb_create(const flb_lattice_desc* desc, flb_lattice** out);
+FLB_API int flb_destroy(flb_lattice* lat);
+
+/* Device bytes held by the handle. */
+FLB_API int flb_memory_bytes(const flb_lattice* lat, size_t* bytes);
+
+/* Flag field (uint8 per cell).  Replaces BlockFieldManager<FLAG>::copyToDevice
+ * (src/data_struct/field_struct.h:176-177). */
+FLB_API int flb_upload_flags(flb_lattice* lat, const uint8_t* host_flags, void* stream);
+FLB_API int flb_download_flags(flb_lattice* lat, uint8_t* host_flags, void* stream);
+
+/* Populations, 19 x N in logical order, host dtype FLB_DTYPE_*.  Replaces
+ * getField<POP<T,19>>() access and copyToDevice/copyToHost of POP. */
+FLB_API int flb_upload_pops(flb_lattice* lat, const void* host, int host_dtype, void* stream);
+FLB_API int flb_download_pops(flb_lattice* lat, void* host, int host_dtype, void* stream);
+
+/* RHO (N) or VELOCITY (3N, AoS) field.  Replaces getField<RHO>/getField<VELOCITY>
+ * with copyToDevice/copyToHost. */
+FLB_API int flb_upload_field(flb_lattice* lat, int field, const void* host, int host_dtype,
+                     void* stream);
+FLB_API int flb_download_field(flb_lattice* lat, int field, void* host, int host_dtype, void* stream);
+
+/* f_i = rho0*w_i on every cell (block_lattice.hh:673-680). */
+FLB_API int flb_init_equilibrium(flb_lattice* lat, double rho0, void* stream);
+
+/* n time steps, each the fused equivalent of
+ *   ApplyCellDynamics<NSTask>(FlagFM); Stream();
+ * (block_lattice.hh:72-92 + 64-70; CUDA twins block_lattice.hh:210-231).
+ * Streaming keeps the reference's periodic wrap over the linear cell index. */
+FLB_API int flb_step(flb_lattice* lat, int nsteps, void* stream);
+
+/* Write RHO and VELOCITY from the current populations on cells whose flag
+ * shares a bit with `key`: ApplyCellDynamics<TaskSelector<Key_TypePair<key,
+ * moment::rhoU<CELL,true>>>> (src/lbm/moment.h:382-398). */
+FLB_API int flb_compute_rhou(flb_lattice* lat, uint8_t key, void* stream);
+
+/* FP64 sums over cells whose flag shares a bit with `key`:
+ * out[0] = sum rho, out[1..3] = sum rho*u (mass and momentum). */
+FLB_API int flb_reduce_conservation(flb_lattice* lat, uint8_t key, double out[4], void* stream);
+
+/* Steady-state check: max |u - u_prev| over cells matching `key` since the
+ * previous call (first call: against u = 0), FP64 reduction.  Replaces
+ * BlockLattice::getToleranceU (block_lattice.hh:266-288). */
+FLB_API int flb_tolerance_u(flb_lattice* lat, uint8_t key, double* max_du, void* stream);
+
+/* Non-finite check of the populations: *bad = number of non-finite values. */
+FLB_API int flb_check_finite(flb_lattice* lat, uint64_t* bad, void* stream);
+
+/* Device pointers for zero-copy consumers: populations (current buffer),
+ * flags, RHO, VELOCITY (SoA planes), with the padded layout
+ * (pitch_x elements per row, rows per plane = ny, plane stride, direction
+ * stride, all in elements). */
+typedef struct flb_layout {
+  int nx, ny, nz;
+  int pitch_x;
+  size_t plane;      /* pitch_x * ny */
+  size_t dir_stride; /* elements between consecutive directions */
+  int elem_bytes;    /* population element size */
+} flb_layout;
+FLB_API int flb_get_layout(const flb_lattice* lat, flb_layout* layout);
+FLB_API int flb_device_pointers(flb_lattice* lat, void** pops, void** flags, void** rho, void** vel);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLB_H_ */

@@ -1,0 +1,239 @@
+// Oracle harness (test infrastructure only): drives the reference FreeLB CPU
+// path, compiled from the reference's own headers, on the lid-driven cavity and
+// dumps what the parity tests compare against.
+//
+// It reproduces benchmarks/cavity3d/cavity3d.cpp:111-223 (flag setup, lattice
+// construction, moving-lid velocity, NSTask = first-matching-key selector over
+// {2: bulk collision, 4: BounceBack, 8: BounceBackMovingWall},
+// ApplyCellDynamics + Stream per step) with lattice parameters taken from the
+// command line instead of an ini file:
+//
+//   ref_cavity <model> <Ni> <RT> <u_lid> <steps> <warmup> <outdir|-> [Cs] [blockfile]
+//
+//   model     bgk | les | mrt
+//             bgk: collision::BGK<moment::rhoU, equilibrium::SecondOrder>
+//             les: collision::SmagorinskyBGK<moment::rhoU<CELL,true>, SecondOrder>
+//                  (rhoU writes RHO, so the RHO field read at collisionLES.h:50
+//                   holds the local density of this step)
+//             mrt: collision::MRT_Feq_RhoU with the D3Q19 basis specialised in
+//                  mrt_d3q19_table.h (the reference ships only D2Q9 data)
+//   Ni        interior cells per axis (stored mesh is (Ni+2)^3, one void layer)
+//   RT        relaxation time tau (lattice units; dx = dt = 1 so u_lid is lattice)
+//   blockfile optional BlockReader file (io/block_reader.h) for a multi-block run;
+//             NormalCommunicate() follows Stream() as in
+//             examples/cavity3d/cavity3d.cpp:220.
+//
+// Output (when outdir != "-"): meta.txt, flags.u8, pops.bin (19 x N, logical
+// order after the PS rotation), rho.bin (N), u.bin (3N, AoS) -- per block with
+// suffix _b<k> -- where rho/u are refreshed on fluid cells with
+// moment::rhoU<CELL,true> after the last step (examples/cavity3d/cavity3d.cpp:191-194).
+// It always prints one line "MLUPS <value> CELLS <n> STEPS <k> SECONDS <t> THREADS <p>"
+// using the reference's Timer (utils/timer.h:50-112).
+
+#include "freelb.h"
+#include "freelb.hh"
+
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <fstream>
+
+#include "mrt_d3q19_table.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+int Thread_Num = 1;
+
+#ifndef REF_T
+#define REF_T float
+#endif
+using T = REF_T;
+using LatSet = D3Q19<T>;
+
+constexpr std::uint8_t VoidFlag = std::uint8_t(1);
+constexpr std::uint8_t AABBFlag = std::uint8_t(2);
+constexpr std::uint8_t BouncebackFlag = std::uint8_t(4);
+constexpr std::uint8_t BBMovingWallFlag = std::uint8_t(8);
+
+struct Params {
+  std::string model;
+  int Ni;
+  T RT;
+  T ulid;
+  int steps;
+  int warmup;
+  std::string outdir;
+  T Cs;
+  std::string blockfile;
+};
+
+template <typename V>
+static void dump(const std::string& path, const V* data, std::size_t n) {
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(data), sizeof(V) * n);
+}
+
+template <typename FIELDS, typename GEO>
+struct Runner {
+  using CELL = Cell<T, LatSet, FIELDS>;
+
+  template <typename BulkPolicy, typename INITVALUES>
+  static void run(const Params& p, GEO& Geo, BaseConverter<T>& BaseConv, INITVALUES& InitValues,
+                  const AABB<T, 3>& cavity, const AABB<T, 3>& toplid) {
+    BlockFieldManager<FLAG, T, 3> FlagFM(Geo, VoidFlag);
+    FlagFM.forEach(cavity, [&](FLAG& field, std::size_t id) { field.SetField(id, AABBFlag); });
+    FlagFM.template SetupBoundary<LatSet>(cavity, BouncebackFlag);
+    FlagFM.forEach(toplid, [&](FLAG& field, std::size_t id) {
+      if (util::isFlag(field.get(id), BouncebackFlag)) field.SetField(id, BBMovingWallFlag);
+    });
+
+    BlockLatticeManager<T, LatSet, FIELDS> NSLattice(Geo, InitValues, BaseConv);
+    Vector<T, 3> U_Wall{p.ulid, T{}, T{}};
+    Vector<T, 3> LatU_Wall = BaseConv.getLatticeU(U_Wall);
+    NSLattice.template getField<VELOCITY<T, LatSet::d>>().forEach(
+      toplid, FlagFM, BBMovingWallFlag,
+      [&](auto& field, std::size_t id) { field.SetField(id, LatU_Wall); });
+
+    using BulkTask = tmp::Key_TypePair<AABBFlag, BulkPolicy>;
+    using BBTask = tmp::Key_TypePair<BouncebackFlag, collision::BounceBack<CELL>>;
+    using BBMVTask = tmp::Key_TypePair<BBMovingWallFlag, collision::BounceBackMovingWall<CELL>>;
+    using NSTask = TaskSelector<std::uint8_t, CELL, BulkTask, BBTask, BBMVTask>;
+    using RhoUtask = tmp::Key_TypePair<AABBFlag, moment::rhoU<CELL, true>>;
+    using RhoUTask = TaskSelector<std::uint8_t, CELL, RhoUtask>;
+
+    const bool multi = Geo.getBlockNum() > 1;
+    for (int i = 0; i < p.warmup; ++i) {
+      NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
+      NSLattice.Stream();
+      if (multi) NSLattice.NormalCommunicate();
+    }
+    Timer MainLoopTimer;
+    MainLoopTimer.START_TIMER();
+    while (MainLoopTimer() < p.steps) {
+      NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
+      NSLattice.Stream();
+      if (multi) NSLattice.NormalCommunicate();
+      ++MainLoopTimer;
+    }
+    MainLoopTimer.END_TIMER();
+    const double ms = double(std::chrono::duration_cast<std::chrono::microseconds>(
+                               MainLoopTimer.END - MainLoopTimer.START).count()) / 1000.0;
+    const double cells = double(Geo.getTotalCellNum());
+    const double mlups = ms > 0 ? double(p.steps) * cells / ms / 1000.0 : 0.0;
+    std::printf("MLUPS %.6f CELLS %.0f STEPS %d SECONDS %.6f THREADS %d\n", mlups, cells,
+                p.steps, ms / 1000.0, Thread_Num);
+
+    if (p.outdir == "-") return;
+    NSLattice.template ApplyCellDynamics<RhoUTask>(FlagFM);
+    {
+      std::ofstream meta(p.outdir + "/meta.txt");
+      meta.precision(17);
+      meta << "model " << p.model << "\nNi " << p.Ni << "\nRT " << p.RT << "\nulid " << p.ulid
+           << "\nsteps " << p.steps << "\nwarmup " << p.warmup << "\nblocks " << Geo.getBlockNum()
+           << "\nsizeofT " << sizeof(T) << "\nomega " << BaseConv.getOMEGA() << "\n";
+      for (int ib = 0; ib < Geo.getBlockNum(); ++ib) {
+        const auto& blk = Geo.getBlock(ib);
+        meta << "block " << ib << " mesh " << blk.getNx() << " " << blk.getNy() << " "
+             << blk.getNz() << " min " << blk.getMin()[0] << " " << blk.getMin()[1] << " "
+             << blk.getMin()[2] << " overlap " << blk.getOverlap() << "\n";
+      }
+    }
+    for (int ib = 0; ib < Geo.getBlockNum(); ++ib) {
+      auto& blat = NSLattice.getBlockLat(ib);
+      const std::size_t N = blat.getN();
+      const std::string sfx = multi ? ("_b" + std::to_string(ib)) : std::string();
+      const auto& flagarr = FlagFM.getBlockField(ib).getField(0);
+      std::vector<std::uint8_t> flags(N);
+      for (std::size_t id = 0; id < N; ++id) flags[id] = flagarr[id];
+      dump(p.outdir + "/flags" + sfx + ".u8", flags.data(), N);
+      std::vector<T> pops(19 * N);
+      auto& popf = blat.template getField<POP<T, LatSet::q>>();
+      for (int i = 0; i < 19; ++i)
+        for (std::size_t id = 0; id < N; ++id) pops[i * N + id] = popf.getField(i)[id];
+      dump(p.outdir + "/pops" + sfx + ".bin", pops.data(), 19 * N);
+      std::vector<T> rho(N), u(3 * N);
+      auto& rhof = blat.template getField<RHO<T>>().getField(0);
+      auto& uf = blat.template getField<VELOCITY<T, LatSet::d>>().getField(0);
+      for (std::size_t id = 0; id < N; ++id) {
+        rho[id] = rhof[id];
+        for (int d = 0; d < 3; ++d) u[3 * id + d] = uf[id][d];
+      }
+      dump(p.outdir + "/rho" + sfx + ".bin", rho.data(), N);
+      dump(p.outdir + "/u" + sfx + ".bin", u.data(), 3 * N);
+    }
+  }
+};
+
+template <typename GEO>
+static void dispatch(const Params& p, GEO& Geo, BaseConverter<T>& BaseConv,
+                     const AABB<T, 3>& cavity, const AABB<T, 3>& toplid) {
+  if (p.model == "bgk") {
+    using FIELDS = TypePack<RHO<T>, VELOCITY<T, LatSet::d>, POP<T, LatSet::q>>;
+    using CELL = Cell<T, LatSet, FIELDS>;
+    ValuePack InitValues(BaseConv.getLatRhoInit(), Vector<T, 3>{}, T{});
+    Runner<FIELDS, GEO>::template run<
+      collision::BGK<moment::rhoU<CELL>, equilibrium::SecondOrder<CELL>>>(
+        p, Geo, BaseConv, InitValues, cavity, toplid);
+  } else if (p.model == "mrt") {
+    using FIELDS = TypePack<RHO<T>, VELOCITY<T, LatSet::d>, POP<T, LatSet::q>>;
+    using CELL = Cell<T, LatSet, FIELDS>;
+    ValuePack InitValues(BaseConv.getLatRhoInit(), Vector<T, 3>{}, T{});
+    Runner<FIELDS, GEO>::template run<collision::MRT_Feq_RhoU<CELL>>(p, Geo, BaseConv,
+                                                                      InitValues, cavity, toplid);
+  } else if (p.model == "les") {
+    using FIELDS =
+      TypePack<RHO<T>, VELOCITY<T, LatSet::d>, POP<T, LatSet::q>, SMAGORINSKY<T>>;
+    using CELL = Cell<T, LatSet, FIELDS>;
+    ValuePack InitValues(BaseConv.getLatRhoInit(), Vector<T, 3>{}, T{}, p.Cs);
+    Runner<FIELDS, GEO>::template run<
+      collision::SmagorinskyBGK<moment::rhoU<CELL, true>, equilibrium::SecondOrder<CELL>>>(
+        p, Geo, BaseConv, InitValues, cavity, toplid);
+  } else {
+    std::fprintf(stderr, "unknown model %s\n", p.model.c_str());
+    std::exit(2);
+  }
+}
+
+int main(int argc, char** argv) {
+  if (argc < 8) {
+    std::fprintf(stderr,
+                 "usage: %s <bgk|les|mrt> <Ni> <RT> <u_lid> <steps> <warmup> <outdir|-> [Cs] "
+                 "[blockfile]\n",
+                 argv[0]);
+    return 2;
+  }
+  Params p;
+  p.model = argv[1];
+  p.Ni = std::atoi(argv[2]);
+  p.RT = T(std::atof(argv[3]));
+  p.ulid = T(std::atof(argv[4]));
+  p.steps = std::atoi(argv[5]);
+  p.warmup = std::atoi(argv[6]);
+  p.outdir = argv[7];
+  p.Cs = argc > 8 ? T(std::atof(argv[8])) : T(0.1);
+  p.blockfile = argc > 9 ? argv[9] : "";
+#ifdef _OPENMP
+  Thread_Num = omp_get_max_threads();
+#endif
+  const T Cell_Len = T(1);
+  // dx = dt = 1: lattice and physical units coincide (unit_converter.h:225-228)
+  BaseConverter<T> BaseConv(LatSet::cs2);
+  BaseConv.SimplifiedConverterFromRT(p.Ni, p.ulid, p.RT);
+
+  const int Ni = p.Ni, Nj = p.Ni, Nk = p.Ni;
+  AABB<T, 3> cavity(Vector<T, 3>{},
+                    Vector<T, 3>(T(Ni * Cell_Len), T(Nj * Cell_Len), T(Nk * Cell_Len)));
+  AABB<T, 3> toplid(Vector<T, 3>(Cell_Len, Cell_Len, T((Nk - 1) * Cell_Len)),
+                    Vector<T, 3>(T((Ni - 1) * Cell_Len), T((Nj - 1) * Cell_Len), T(Nk * Cell_Len)));
+  if (p.blockfile.empty()) {
+    BlockGeometry3D<T> Geo(Ni, Nj, Nk, 1, cavity, Cell_Len);
+    dispatch(p, Geo, BaseConv, cavity, toplid);
+  } else {
+    BlockReader<T, 3> reader(p.blockfile);
+    BlockGeometry3D<T> Geo(reader, true);
+    dispatch(p, Geo, BaseConv, cavity, toplid);
+  }
+  return 0;
+}

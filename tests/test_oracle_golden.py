@@ -1,0 +1,97 @@
+"""CPU tests: pin the oracle restatement (oracle/flb_oracle.c) to the reference.
+
+The golden fixtures are outputs of the reference's own CPU path
+(tests/golden/make_golden.py).  When the reference harness is built
+(oracle/_ref, only where the reference sources exist) the restatement is also
+checked against live reference runs.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_maxnorm
+from oracle import oracle as O
+
+SMALL = ["cavity_bgk_f32_n10_s40", "cavity_bgk_f64_n10_s40", "cavity_les_f32_n10_s40",
+         "cavity_les_f64_n10_s40", "cavity_mrt_f32_n10_s40", "cavity_mrt_f64_n10_s40",
+         "cavity_bgk_f32_n7_s200"]
+
+
+def run_oracle(model, ni, tau, ulid, steps, cs, dtype):
+    lat = O.cavity(int(ni), model=model, tau=tau, ulid=ulid, cs=cs, dtype=dtype)
+    lat.step(int(steps))
+    rho, u = lat.rhou_fields()
+    return lat, rho, u
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_restatement_matches_reference_golden(name):
+    g = golden(name)
+    ni, tau, ulid, steps, cs = g["params"]
+    model = str(g["model"])
+    dtype = np.float64 if "f64" in name else np.float32
+    lat, rho, u = run_oracle(model, ni, tau, ulid, steps, cs, dtype)
+    assert np.array_equal(lat.flags, g["flags"]), "flags must be bit-exact"
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    assert rel_maxnorm(lat.pops, g["pops"]) < tol
+    assert rel_maxnorm(rho, g["rho"]) < tol
+    assert rel_maxnorm(u, g["u"]) < tol
+
+
+def test_restatement_c1_benchmark_shape():
+    """100^3 cavity, tau=0.53, u_lid=0.1, 1000 steps (reference cavity3d shape)."""
+    g = golden("c1_bgk_f32_n100_s1000")
+    lat, rho, u = run_oracle("bgk", 100, 0.53, 0.1, 1000, 0.1, np.float32)
+    n = 102
+    assert np.array_equal(lat.flags, g["flags"])
+    pops = lat.pops.reshape(19, n, n, n)
+    sums = pops.astype(np.float64).sum(axis=(1, 2, 3))
+    assert np.max(np.abs(sums - g["pop_sums"]) / np.abs(g["pop_sums"])) < 1e-6
+    assert rel_maxnorm(pops[:, :, n // 2, :], g["pops_plane"]) < 1e-5
+    assert rel_maxnorm(u.reshape(n, n, n, 3)[:, n // 2], g["u_plane"]) < 1e-5
+    assert rel_maxnorm(rho.reshape(n, n, n)[:, n // 2], g["rho_plane"]) < 1e-5
+
+
+@pytest.mark.parametrize("ni", [4, 9, 16])
+def test_cavity_flags_restatement(ni):
+    """oracle_cavity_flags against the analytic layout, and the product helper."""
+    import freelb_b200
+    f = O.cavity_flags(ni)
+    assert np.array_equal(f, freelb_b200.cavity_flags(ni))
+    n = ni + 2
+    v = f.reshape(n, n, n)
+    assert (v[0] == 1).all() and (v[-1] == 1).all()
+    assert (v[n - 2, 2:n - 2, 2:n - 2] == 8).all()
+    assert int((f == 2).sum()) == (ni - 2) ** 3
+
+
+def test_task_lut_first_match():
+    lut = O.task_lut([2, 4 | 8, 8], [O.OP_BULK, O.OP_BB, O.OP_MBB])
+    assert lut[2] == O.OP_BULK and lut[4] == O.OP_BB
+    assert lut[8] == O.OP_BB          # first key sharing a bit wins (tmp.h:283-309)
+    assert lut[1] == O.OP_NONE and lut[6] == O.OP_BULK
+
+
+def test_ps_streaming_is_linear_periodic_shift():
+    """With no collision, one step shifts every direction array by Delta_i mod N."""
+    nx, ny, nz = 5, 4, 3
+    N = nx * ny * nz
+    flags = np.ones(N, dtype=np.uint8)
+    lat = O.Lattice(nx, ny, nz, flags, dtype=np.float64)
+    rng = np.random.default_rng(0)
+    lat.pops[:] = rng.random(19 * N)
+    before = lat.pops.reshape(19, N).copy()
+    lat.step(1)
+    after = lat.pops.reshape(19, N)
+    for i in range(19):
+        d = O.C[i, 0] + O.C[i, 1] * nx + O.C[i, 2] * nx * ny
+        assert np.array_equal(after[i], np.roll(before[i], d))
+
+
+@pytest.mark.skipif(O.ref_binary() is None, reason="reference harness not built here")
+@pytest.mark.parametrize("model", ["bgk", "les", "mrt"])
+def test_restatement_matches_live_reference(model):
+    r = O.run_reference(model, 14, 0.52, 0.08, 60, 0, cs=0.12, dtype=np.float64, threads=2)
+    lat, rho, u = run_oracle(model, 14, 0.52, 0.08, 60, 0.12, np.float64)
+    assert np.array_equal(lat.flags, r["flags"])
+    assert rel_maxnorm(lat.pops, r["pops"]) < 1e-12
+    assert rel_maxnorm(u, r["u"]) < 1e-12

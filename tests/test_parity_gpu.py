@@ -1,0 +1,165 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference.
+
+Ground truth is (a) the golden fixtures produced by the reference's own CPU
+code and (b) the oracle restatement, itself pinned to the reference by
+tests/test_oracle_golden.py.  Tolerances: relative max-norm 1e-5 for FP32
+(populations, rho, u), 1e-12 for FP64; flags bit-exact.
+"""
+import numpy as np
+import pytest
+
+import freelb_b200 as F
+from conftest import golden, rel_l2, rel_maxnorm
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SMALL = ["cavity_bgk_f32_n10_s40", "cavity_bgk_f64_n10_s40", "cavity_les_f32_n10_s40",
+         "cavity_les_f64_n10_s40", "cavity_mrt_f32_n10_s40", "cavity_mrt_f64_n10_s40",
+         "cavity_bgk_f32_n7_s200"]
+
+
+def gpu_cavity(model, ni, tau, ulid, steps, cs, storage):
+    lat = F.cavity(int(ni), tau=tau, ulid=ulid, storage=storage, model=model, smagorinsky=cs)
+    lat.step(int(steps))
+    rho, u = lat.rhou(key=2)
+    return lat, rho, u
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_gpu_matches_reference_golden(gpu_ok, name):
+    g = golden(name)
+    ni, tau, ulid, steps, cs = g["params"]
+    model = str(g["model"])
+    storage = "fp64" if "f64" in name else "fp32"
+    lat, rho, u = gpu_cavity(model, ni, tau, ulid, steps, cs, storage)
+    assert np.array_equal(lat.download_flags(), g["flags"])
+    tol = 1e-12 if storage == "fp64" else 1e-5
+    pops = lat.download_pops()
+    assert rel_maxnorm(pops, g["pops"]) < tol       # every cell, void layer included
+    assert rel_maxnorm(rho, g["rho"]) < tol
+    assert rel_maxnorm(u, g["u"]) < tol
+
+
+def test_gpu_c1_benchmark_shape(gpu_ok):
+    """Reference cavity3d shape: 100^3, tau=0.53, u_lid=0.1, 1000 steps, FP32."""
+    g = golden("c1_bgk_f32_n100_s1000")
+    lat, rho, u = gpu_cavity("bgk", 100, 0.53, 0.1, 1000, 0.1, "fp32")
+    n = 102
+    assert np.array_equal(lat.download_flags(), g["flags"])
+    pops = lat.download_pops().reshape(19, n, n, n)
+    sums = pops.astype(np.float64).sum(axis=(1, 2, 3))
+    assert np.max(np.abs(sums - g["pop_sums"]) / np.abs(g["pop_sums"])) < 1e-6
+    assert rel_maxnorm(pops[:, :, n // 2, :], g["pops_plane"]) < 1e-5
+    assert rel_maxnorm(u.reshape(n, n, n, 3)[:, n // 2], g["u_plane"]) < 1e-5
+    assert rel_maxnorm(rho.reshape(n, n, n)[:, n // 2], g["rho_plane"]) < 1e-5
+    # full arrays against the oracle restatement
+    ol = O.cavity(100, tau=0.53, ulid=0.1)
+    ol.step(1000)
+    orho, ou = ol.rhou_fields()
+    assert rel_maxnorm(pops.reshape(-1), ol.pops) < 1e-5
+    assert rel_maxnorm(rho, orho) < 1e-5
+    assert rel_maxnorm(u, ou) < 1e-5
+
+
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+@pytest.mark.parametrize("shape", [(37, 5, 9), (70, 33, 12), (6, 40, 7)])
+def test_gpu_vs_oracle_random_flags_fp64(gpu_ok, model, shape):
+    """Non-cubic meshes (pitch padding), every op, random first-match task list."""
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    rng = np.random.default_rng(nx * 100 + ny)
+    flags = rng.choice(np.array([1, 2, 4, 8, 16, 2 | 16, 32], dtype=np.uint8), size=N,
+                       p=[.1, .5, .1, .1, .1, .05, .05])
+    keys, ops = (2, 4, 8, 16), ("bulk", "bounceback", "movingwall", "field_bgk")
+    tasks = tuple(zip(keys, ops))
+    lat = F.Lattice(nx, ny, nz, 0.57, storage="fp64", model=model, smagorinsky=0.15,
+                    mrt_rate=1.1, tasks=tasks)
+    ref = O.Lattice(nx, ny, nz, flags, model=model, tau=0.57, cs=0.15, mrt_rate=1.1,
+                    dtype=np.float64, keys=keys,
+                    ops=(O.OP_BULK, O.OP_BB, O.OP_MBB, O.OP_FIELD_BGK))
+    pops0 = (ref.pops.reshape(19, N) * (1 + 0.05 * rng.standard_normal((19, N)))).reshape(-1)
+    ref.pops[:] = pops0
+    ref.rho[:] = 1 + 0.01 * rng.standard_normal(N)
+    ref.u[:] = 0.03 * rng.standard_normal(3 * N)
+    lat.upload_flags(flags)
+    lat.upload_pops(pops0)
+    lat.upload_field("rho", ref.rho)
+    lat.upload_field("u", ref.u)
+    lat.step(7)
+    ref.step(7)
+    assert rel_maxnorm(lat.download_pops(), ref.pops) < 1e-12
+
+
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+def test_gpu_vs_oracle_fp32_cavity(gpu_ok, model):
+    lat, rho, u = gpu_cavity(model, 24, 0.52, 0.1, 150, 0.1, "fp32")
+    ol = O.cavity(24, model=model, tau=0.52, ulid=0.1, cs=0.1)
+    ol.step(150)
+    orho, ou = ol.rhou_fields()
+    assert rel_maxnorm(lat.download_pops(), ol.pops) < 1e-5
+    assert rel_maxnorm(u, ou) < 1e-5
+    assert rel_maxnorm(rho, orho) < 1e-5
+
+
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+def test_fp16s_velocity_error_vs_fp64(gpu_ok, model):
+    """FP16 storage of f_i - w_i with FP32 arithmetic: relative L2 velocity error
+    against an FP64 run of the same kernel stays below 1e-3."""
+    tau = 0.53 if model != "les" else 0.51
+    runs = {}
+    for storage in ("fp64", "fp16s", "fp32"):
+        lat, rho, u = gpu_cavity(model, 48, tau, 0.1, 600, 0.1, storage)
+        runs[storage] = u.astype(np.float64)
+        assert lat.nonfinite() == 0
+    e16 = rel_l2(runs["fp16s"], runs["fp64"])
+    e32 = rel_l2(runs["fp32"], runs["fp64"])
+    assert e16 < 1e-3, e16
+    assert e32 < 1e-5, e32
+
+
+def test_pops_roundtrip_and_layout(gpu_ok):
+    nx, ny, nz = 45, 7, 6
+    N = nx * ny * nz
+    rng = np.random.default_rng(3)
+    for storage, dt in (("fp32", np.float32), ("fp64", np.float64), ("fp16s", np.float32)):
+        lat = F.Lattice(nx, ny, nz, 0.6, storage=storage)
+        w = np.repeat(O.W, N)
+        p = (w * (1 + 0.1 * rng.standard_normal(19 * N))).astype(dt)
+        lat.upload_pops(p)
+        back = lat.download_pops(dt)
+        if storage == "fp16s":
+            # binary16 keeps 11 significant bits of (f - w): half-ulp relative bound
+            bound = 2.0 ** -11 * np.abs(p.astype(np.float64) - w) + 1e-7
+            assert np.all(np.abs(back.astype(np.float64) - p) <= bound)
+        else:
+            assert np.array_equal(back, p)
+        L = lat.layout()
+        assert L.pitch_x % 32 == 0 and L.pitch_x >= nx and L.dir_stride % 64 == 0
+        f = rng.integers(0, 255, N, dtype=np.uint8)
+        lat.upload_flags(f)
+        assert np.array_equal(lat.download_flags(), f)
+        r = rng.random(N).astype(dt)
+        lat.upload_field("rho", r)
+        assert np.array_equal(lat.download_field("rho", dt), r)
+        v = rng.random(3 * N).astype(dt)
+        lat.upload_field("u", v)
+        assert np.array_equal(lat.download_field("u", dt), v)
+
+
+def test_conservation_and_tolerance(gpu_ok):
+    lat = F.cavity(20, tau=0.55, ulid=0.1, storage="fp64")
+    lat.step(30)
+    pops = lat.download_pops().reshape(19, -1)
+    flags = lat.download_flags()
+    m = (flags & 2) != 0
+    s = lat.conservation(key=2)
+    assert abs(s[0] - pops[:, m].sum()) < 1e-9
+    assert abs(s[1] - (O.C[:, 0:1] * pops[:, m]).sum()) < 1e-9
+    rho, u = lat.rhou(key=2)
+    t1 = lat.tolerance_u(key=2)
+    assert abs(t1 - np.abs(u.reshape(-1, 3)[m]).max()) < 1e-12
+    assert lat.tolerance_u(key=2) == 0.0
+    lat.step(1)
+    assert lat.tolerance_u(key=2) > 0.0
+    assert lat.nonfinite() == 0
