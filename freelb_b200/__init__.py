@@ -62,19 +62,55 @@ def make_desc(nx, ny, nz, tau, storage="fp32", model="bgk", smagorinsky=0.1, mrt
 
 
 class Lattice:
-    """One device-resident D3Q19 block lattice (BlockLattice on the GPU)."""
+    """Device-resident D3Q19 lattice: one block (BlockLattice) or several blocks
+    (BlockLatticeManager) advanced together.
+
+    Single block:  Lattice(nx, ny, nz, tau, ...)
+    Blocks:        Lattice.blocks([(nx, ny, nz, ox, oy, oz[, omega]), ...], tau, mode=...)
+    Transfer methods take ``block=`` (default 0).
+    """
 
     def __init__(self, nx, ny, nz, tau, storage="fp32", model="bgk", smagorinsky=0.1,
-                 mrt_rate=1.2, rho0=1.0, tasks=CAVITY_TASKS, omega=None):
-        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
-        self.N = self.nx * self.ny * self.nz
+                 mrt_rate=1.2, rho0=1.0, tasks=CAVITY_TASKS, omega=None, _blocks=None,
+                 _mode=None):
         self.storage = storage
+        self.real = np.float64 if storage == "fp64" else np.float32
         self.desc = make_desc(nx, ny, nz, tau, storage, model, smagorinsky, mrt_rate, rho0,
                               tasks, omega)
         h = ctypes.c_void_p()
-        C.call("flb_create", ctypes.byref(self.desc), ctypes.byref(h))
+        if _blocks is None:
+            C.call("flb_create", ctypes.byref(self.desc), ctypes.byref(h))
+            self.shapes = [(int(nx), int(ny), int(nz))]
+        else:
+            arr = (C.BlockDesc * len(_blocks))()
+            for k, b in enumerate(_blocks):
+                arr[k].nx, arr[k].ny, arr[k].nz = int(b[0]), int(b[1]), int(b[2])
+                arr[k].ox, arr[k].oy, arr[k].oz = int(b[3]), int(b[4]), int(b[5])
+                arr[k].omega = float(b[6]) if len(b) > 6 else 0.0
+            C.call("flb_create_blocks", ctypes.byref(self.desc), len(_blocks), arr,
+                   int(_mode), ctypes.byref(h))
+            self.shapes = [(int(b[0]), int(b[1]), int(b[2])) for b in _blocks]
         self._h = h
-        self.real = np.float64 if storage == "fp64" else np.float32
+        self.nx, self.ny, self.nz = self.shapes[0]
+        self.N = self.nx * self.ny * self.nz
+
+    @classmethod
+    def blocks(cls, blocks, tau, mode="halo", **kw):
+        m = C.BLOCKS_HALO if mode == "halo" else C.BLOCKS_INDEPENDENT
+        return cls(3, 3, 3, tau, _blocks=blocks, _mode=m, **kw)
+
+    @property
+    def nblocks(self):
+        return len(self.shapes)
+
+    def ncells(self, block=0):
+        nx, ny, nz = self.shapes[block]
+        return nx * ny * nz
+
+    def halo_count(self):
+        v = ctypes.c_longlong()
+        C.call("flb_halo_count", self._h, ctypes.byref(v))
+        return int(v.value)
 
     # -- lifetime
     def close(self):
@@ -95,59 +131,78 @@ class Lattice:
         self.close()
 
     # -- transfers
-    def upload_flags(self, flags, stream=None):
+    def upload_flags(self, flags, stream=None, block=0):
         f = np.ascontiguousarray(flags, dtype=np.uint8).reshape(-1)
-        assert f.size == self.N
-        C.call("flb_upload_flags", self._h, _ptr(f), _stream(stream))
+        assert f.size == self.ncells(block)
+        C.call("flb_upload_flags_block", self._h, block, _ptr(f), _stream(stream))
 
-    def download_flags(self, stream=None):
-        f = np.empty(self.N, dtype=np.uint8)
-        C.call("flb_download_flags", self._h, _ptr(f), _stream(stream))
+    def download_flags(self, stream=None, block=0):
+        f = np.empty(self.ncells(block), dtype=np.uint8)
+        C.call("flb_download_flags_block", self._h, block, _ptr(f), _stream(stream))
         return f
 
-    def upload_pops(self, pops, stream=None):
+    def upload_pops(self, pops, stream=None, block=0):
         p = np.ascontiguousarray(pops).reshape(-1)
-        assert p.size == 19 * self.N
+        assert p.size == 19 * self.ncells(block)
         dt = C.DTYPE_F64 if p.dtype == np.float64 else C.DTYPE_F32
         p = p.astype(np.float64 if dt == C.DTYPE_F64 else np.float32, copy=False)
-        C.call("flb_upload_pops", self._h, _ptr(p), dt, _stream(stream))
+        C.call("flb_upload_pops_block", self._h, block, _ptr(p), dt, _stream(stream))
 
-    def download_pops(self, dtype=None, stream=None):
+    def download_pops(self, dtype=None, stream=None, block=0):
         dtype = np.dtype(dtype or self.real)
-        p = np.empty(19 * self.N, dtype=dtype)
+        p = np.empty(19 * self.ncells(block), dtype=dtype)
         dt = C.DTYPE_F64 if dtype == np.float64 else C.DTYPE_F32
-        C.call("flb_download_pops", self._h, _ptr(p), dt, _stream(stream))
+        C.call("flb_download_pops_block", self._h, block, _ptr(p), dt, _stream(stream))
         return p
 
-    def upload_field(self, name, values, stream=None):
+    def upload_field(self, name, values, stream=None, block=0):
         fid = C.FIELD_RHO if name == "rho" else C.FIELD_VELOCITY
+        n = self.ncells(block)
         v = np.ascontiguousarray(values).reshape(-1)
-        assert v.size == (self.N if fid == C.FIELD_RHO else 3 * self.N)
+        assert v.size == (n if fid == C.FIELD_RHO else 3 * n)
         dt = C.DTYPE_F64 if v.dtype == np.float64 else C.DTYPE_F32
         v = v.astype(np.float64 if dt == C.DTYPE_F64 else np.float32, copy=False)
-        C.call("flb_upload_field", self._h, fid, _ptr(v), dt, _stream(stream))
+        C.call("flb_upload_field_block", self._h, block, fid, _ptr(v), dt, _stream(stream))
 
-    def download_field(self, name, dtype=None, stream=None):
+    def download_field(self, name, dtype=None, stream=None, block=0):
         fid = C.FIELD_RHO if name == "rho" else C.FIELD_VELOCITY
         dtype = np.dtype(dtype or self.real)
-        v = np.empty(self.N if fid == C.FIELD_RHO else 3 * self.N, dtype=dtype)
+        n = self.ncells(block)
+        v = np.empty(n if fid == C.FIELD_RHO else 3 * n, dtype=dtype)
         dt = C.DTYPE_F64 if dtype == np.float64 else C.DTYPE_F32
-        C.call("flb_download_field", self._h, fid, _ptr(v), dt, _stream(stream))
+        C.call("flb_download_field_block", self._h, block, fid, _ptr(v), dt, _stream(stream))
         return v
 
     # -- compute
     def init_equilibrium(self, rho0=1.0, stream=None):
         C.call("flb_init_equilibrium", self._h, float(rho0), _stream(stream))
 
-    def step(self, n=1, stream=None):
-        C.call("flb_step", self._h, int(n), _stream(stream))
+    def step(self, n=1, stream=None, graph=False):
+        C.call("flb_step_graph" if graph else "flb_step", self._h, int(n), _stream(stream))
+
+    def set_launch(self, tile_y=8, ctas_per_sm=0):
+        C.call("flb_set_launch", self._h, int(tile_y), int(ctas_per_sm))
+
+    def get_launch(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        C.call("flb_get_launch", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def autotune(self, trial_steps=4, stream=None):
+        """Pick the fastest launch shape; returns (tile_y, ctas_per_sm, ms/step, steps run)."""
+        ty, c, steps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_double()
+        C.call("flb_autotune", self._h, int(trial_steps), _stream(stream), ctypes.byref(ty),
+               ctypes.byref(c), ctypes.byref(ms), ctypes.byref(steps))
+        return ty.value, c.value, ms.value, steps.value
 
     def compute_rhou(self, key=2, stream=None):
         C.call("flb_compute_rhou", self._h, int(key), _stream(stream))
 
-    def rhou(self, key=2, dtype=None, stream=None):
+    def rhou(self, key=2, dtype=None, stream=None, block=0):
         self.compute_rhou(key, stream)
-        return self.download_field("rho", dtype, stream), self.download_field("u", dtype, stream)
+        return (self.download_field("rho", dtype, stream, block),
+                self.download_field("u", dtype, stream, block))
 
     def conservation(self, key=0xFF, stream=None):
         out = (ctypes.c_double * 4)()

@@ -32,6 +32,15 @@ class LatticeDesc(ctypes.Structure):
                 ("task_ops", ctypes.c_uint8 * MAX_TASKS)]
 
 
+class BlockDesc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("ox", ctypes.c_int), ("oy", ctypes.c_int), ("oz", ctypes.c_int),
+                ("omega", ctypes.c_double)]
+
+
+BLOCKS_INDEPENDENT, BLOCKS_HALO = 0, 1
+
+
 class Layout(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("pitch_x", ctypes.c_int), ("plane", ctypes.c_size_t),
@@ -69,6 +78,21 @@ SIGNATURES = {
     "flb_get_layout": [_P, ctypes.POINTER(Layout)],
     "flb_device_pointers": [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P),
                             ctypes.POINTER(_P)],
+    "flb_create_blocks": [ctypes.POINTER(LatticeDesc), _I, ctypes.POINTER(BlockDesc), _I,
+                          ctypes.POINTER(_P)],
+    "flb_block_count": [_P, ctypes.POINTER(_I)],
+    "flb_halo_count": [_P, ctypes.POINTER(ctypes.c_longlong)],
+    "flb_upload_flags_block": [_P, _I, _P, _P],
+    "flb_download_flags_block": [_P, _I, _P, _P],
+    "flb_upload_pops_block": [_P, _I, _P, _I, _P],
+    "flb_download_pops_block": [_P, _I, _P, _I, _P],
+    "flb_upload_field_block": [_P, _I, _I, _P, _I, _P],
+    "flb_download_field_block": [_P, _I, _I, _P, _I, _P],
+    "flb_set_launch": [_P, _I, _I],
+    "flb_get_launch": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)],
+    "flb_step_graph": [_P, _I, _P],
 }
 _RESTYPES = {"flb_last_error": ctypes.c_char_p}
 

@@ -1,18 +1,24 @@
 // flb_api.cu -- the extern "C" boundary (include/flb.h) over the sm_100a kernels.
 //
-// A handle owns the device state of one block lattice: two population buffers
-// (ping-pong), the flag field, the RHO and VELOCITY fields, a 64-byte result
-// word area for reductions and, on first use, a staging buffer for host
-// transfers.  The C++17 classes in freelb_b200/cpp/freelb.h and the Python
-// module call only these functions.
+// A handle owns the device state of one lattice made of one or more blocks:
+// two population buffers (ping-pong), the flag field, the RHO and VELOCITY
+// fields, a 64-byte result area for reductions, the block table and halo
+// records, and, on first use, a staging buffer for host transfers and the
+// captured CUDA graphs.  Blocks are packed one after another inside every
+// direction array (each block padded to pitch = nx rounded up to 32 and to a
+// multiple of 64 elements).  The C++17 classes in freelb_b200/cpp/freelb.h and
+// the Python module call only these functions.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
+#include <vector>
 
 #include "../../include/flb.h"
 #include "flb_kernels.cuh"
@@ -42,30 +48,64 @@ int fail(int code, const char* fmt, ...) {
                   __LINE__);                                                             \
   } while (0)
 
+#define FLB_TRY(expr)      \
+  do {                     \
+    int rc_ = (expr);      \
+    if (rc_) return rc_;   \
+  } while (0)
+
 inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+struct HostBlock {
+  LayoutParams L;   // this block's layout; L.dstride is the handle's direction stride
+  long long base;   // element offset of the block inside every direction array
+  int ox, oy, oz;   // global stored index of local (0,0,0)
+  double omega;     // 1/tau in the arithmetic type
+  long long padded() const { return L.plane * L.nz; }
+};
 
 }  // namespace
 
 struct flb_lattice {
   flb_lattice_desc desc;
   int device = 0;
-  LayoutParams L{};
-  int elem_bytes = 4;   // population element
-  int real_bytes = 4;   // field / arithmetic element
+  int sm_count = 148;
+  int mode = -1;  // -1: single block (flb_create)
+  std::vector<HostBlock> blocks;
+  long long dstride = 0;
+  int elem_bytes = 4;
+  int real_bytes = 4;
   void* pops[2] = {nullptr, nullptr};
   int cur = 0;
   uint8_t* flags = nullptr;
   void* rho = nullptr;
   void* vel = nullptr;
-  double* acc = nullptr;   // 64 bytes of reduction results
-  void* stage = nullptr;   // host-transfer staging, lazily allocated
+  double* acc = nullptr;
+  void* stage = nullptr;
   size_t stage_bytes = 0;
-  double* uprev = nullptr; // tolerance history (3 planes), lazily allocated
+  double* uprev = nullptr;
   StepParams sp{};
-  int block_y = 8;
+  // multi-block launch data
+  BlockEntry* d_blocks = nullptr;
+  long long ntiles = 0;
+  int table_tile_y = 0;
+  HaloRec* d_halo = nullptr;
+  long long nhalo = 0;
+  int tile_y = 8;
+  int ctas_per_sm = 0;
+  // CUDA graphs of the two-step cycle, one per starting buffer parity
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
 };
 
 namespace {
+
+void drop_graphs(flb_lattice* h) {
+  for (auto& g : h->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
 
 int ensure_stage(flb_lattice* h, size_t bytes) {
   if (h->stage_bytes >= bytes) return FLB_OK;
@@ -83,14 +123,8 @@ int grid_1d(long long n) {
   return int(b < 1 ? 1 : b);
 }
 
-int validate_desc(const flb_lattice_desc* d) {
+int validate_common(const flb_lattice_desc* d) {
   if (!d) return fail(FLB_ERR_INVALID, "null descriptor");
-  if (d->nx < 3 || d->ny < 3 || d->nz < 3)
-    return fail(FLB_ERR_INVALID, "mesh %dx%dx%d: each axis needs >= 3 stored cells", d->nx,
-                d->ny, d->nz);
-  if (d->nz > 65535) return fail(FLB_ERR_INVALID, "nz %d exceeds 65535", d->nz);
-  if ((long long)d->nx * d->ny > (1LL << 30))
-    return fail(FLB_ERR_INVALID, "nx*ny too large");
   if (d->storage < 0 || d->storage > 2) return fail(FLB_ERR_INVALID, "bad storage %d", d->storage);
   if (d->model < 0 || d->model > 2) return fail(FLB_ERR_INVALID, "bad model %d", d->model);
   if (!(d->omega > 0.0 && d->omega < 2.0))
@@ -100,10 +134,20 @@ int validate_desc(const flb_lattice_desc* d) {
   for (int t = 0; t < d->ntasks; ++t)
     if (d->task_ops[t] > FLB_OP_FIELD_BGK)
       return fail(FLB_ERR_INVALID, "task %d has unknown op %d", t, d->task_ops[t]);
-  if (d->storage == FLB_STORAGE_FP16S && d->model != FLB_MODEL_BGK && d->model != FLB_MODEL_MRT &&
-      d->model != FLB_MODEL_LES)
-    return fail(FLB_ERR_UNSUPPORTED, "model not built for FP16S");
   return FLB_OK;
+}
+
+int validate_block(int nx, int ny, int nz) {
+  if (nx < 3 || ny < 3 || nz < 3)
+    return fail(FLB_ERR_INVALID, "mesh %dx%dx%d: each axis needs >= 3 stored cells", nx, ny, nz);
+  if (nz > 65535) return fail(FLB_ERR_INVALID, "nz %d exceeds 65535", nz);
+  if ((long long)nx * ny > (1LL << 30)) return fail(FLB_ERR_INVALID, "nx*ny too large");
+  return FLB_OK;
+}
+
+double arith_omega(const flb_lattice_desc& d, double omega) {
+  // BlockLattice stores Omega as T (block_lattice.hh:27-35)
+  return d.storage == FLB_STORAGE_FP64 ? omega : double(float(omega));
 }
 
 // Parameters shared by every kernel of the handle.
@@ -111,28 +155,23 @@ void build_params(flb_lattice* h) {
   const flb_lattice_desc& d = h->desc;
   StepParams& p = h->sp;
   std::memset(&p, 0, sizeof p);
+  const HostBlock& b0 = h->blocks[0];
   p.flags = h->flags;
   p.rho = h->rho;
   p.vel = h->vel;
-  p.nx = d.nx;
-  p.ny = d.ny;
-  p.nz = d.nz;
-  p.pitch = h->L.pitch;
-  p.plane = h->L.plane;
-  p.dstride = h->L.dstride;
-  p.ncells = (long long)d.nx * d.ny * d.nz;
-  for (int i = 0; i < Q; ++i) {
-    p.delta[i] = cx(i) + (long long)cy(i) * d.nx + (long long)cz(i) * d.nx * d.ny;
-    p.off[i] = cx(i) + (long long)cy(i) * p.pitch + (long long)cz(i) * p.plane;
-  }
+  p.nx = b0.L.nx;
+  p.ny = b0.L.ny;
+  p.nz = b0.L.nz;
+  p.pitch = b0.L.pitch;
+  p.plane = b0.L.plane;
+  p.dstride = h->dstride;
   p.ntasks = d.ntasks;
   for (int t = 0; t < d.ntasks; ++t) {
     p.keys[t] = d.task_keys[t];
     p.ops[t] = d.task_ops[t];
   }
   const bool dbl = d.storage == FLB_STORAGE_FP64;
-  // omega in the arithmetic type, as BlockLattice stores T(Conv.getOMEGA())
-  p.omega = dbl ? d.omega : double(float(d.omega));
+  p.omega = arith_omega(d, d.omega);
   const double cs = dbl ? d.smagorinsky : double(float(d.smagorinsky));
   // collisionLES.h:45: Cs*Cs*InvCs2*InvCs2*2 in T, times std::sqrt(2) in double
   const double prod = dbl ? cs * cs * 3.0 * 3.0 * 2.0
@@ -140,7 +179,6 @@ void build_params(flb_lattice* h) {
   p.cs_coeff = prod * std::sqrt(2.0);
   for (int k = 0; k < Q; ++k) {
     double s = d.mrt_rates[k];
-    if (mrt_shear(k)) s = p.omega;
     if (mrt_conserved(k)) s = 0.0;
     p.s_over_norm[k] = s / double(mrt_norm(k));
   }
@@ -154,108 +192,91 @@ void build_params(flb_lattice* h) {
   p.inv_scale = 1.0f / 1024.0f;
 }
 
-template <typename S, typename R>
-int launch_step_t(flb_lattice* h, int nsteps, cudaStream_t st) {
-  const dim3 block(32, h->block_y);
-  const dim3 grid(h->L.pitch / 32, (h->desc.ny + h->block_y - 1) / h->block_y, h->desc.nz);
-  for (int s = 0; s < nsteps; ++s) {
-    h->sp.src = h->pops[h->cur];
-    h->sp.dst = h->pops[h->cur ^ 1];
-    switch (h->desc.model) {
-      case FLB_MODEL_BGK: k_stream_collide<S, R, MODEL_BGK><<<grid, block, 0, st>>>(h->sp); break;
-      case FLB_MODEL_MRT: k_stream_collide<S, R, MODEL_MRT><<<grid, block, 0, st>>>(h->sp); break;
-      default: k_stream_collide<S, R, MODEL_LES><<<grid, block, 0, st>>>(h->sp); break;
-    }
-    h->cur ^= 1;
+// Block table for the tile kernel (rebuilt when tile_y changes).
+int upload_block_table(flb_lattice* h) {
+  if (h->d_blocks && h->table_tile_y == h->tile_y) return FLB_OK;
+  std::vector<BlockEntry> t(h->blocks.size());
+  long long start = 0;
+  for (size_t b = 0; b < h->blocks.size(); ++b) {
+    const HostBlock& hb = h->blocks[b];
+    BlockEntry& e = t[b];
+    e.g = Geom{hb.L.nx, hb.L.ny, hb.L.nz, hb.L.pitch, hb.L.plane, hb.base};
+    e.omega = hb.omega;
+    e.tiles_x = hb.L.pitch / 32;
+    e.tiles_y = (hb.L.ny + h->tile_y - 1) / h->tile_y;
+    e.tile_start = start;
+    start += (long long)e.tiles_x * e.tiles_y * hb.L.nz;
   }
-  FLB_CUDA(cudaGetLastError());
+  if (!h->d_blocks) FLB_CUDA(cudaMalloc((void**)&h->d_blocks, t.size() * sizeof(BlockEntry)));
+  FLB_CUDA(cudaMemcpy(h->d_blocks, t.data(), t.size() * sizeof(BlockEntry),
+                      cudaMemcpyHostToDevice));
+  h->ntiles = start;
+  h->table_tile_y = h->tile_y;
   return FLB_OK;
 }
 
-template <typename S, typename R, typename H>
-int pops_transfer(flb_lattice* h, void* host, bool upload, cudaStream_t st) {
-  const LayoutParams& L = h->L;
-  const size_t hb = sizeof(H);
-  const size_t N = size_t(L.nx) * L.ny * L.nz;
-  const bool direct = sizeof(S) == sizeof(H) && std::is_same<S, H>::value;
-  if (!direct) {
-    int rc = ensure_stage(h, size_t(L.dstride) * sizeof(H));
-    if (rc) return rc;
+// Halo records: every overlap cell of block b owned by a neighbour's interior
+// receives, from that neighbour cell, the populations pointing into b across
+// each face it lies beyond (union over axes: getCommPopDir, communicator.h:76).
+int build_halo(flb_lattice* h) {
+  const int nb = int(h->blocks.size());
+  int gx = 0, gy = 0, gz = 0;
+  for (const HostBlock& b : h->blocks) {
+    if (b.ox < 0 || b.oy < 0 || b.oz < 0)
+      return fail(FLB_ERR_INVALID, "block origin must be non-negative");
+    gx = std::max(gx, b.ox + b.L.nx);
+    gy = std::max(gy, b.oy + b.L.ny);
+    gz = std::max(gz, b.oz + b.L.nz);
   }
-  S* pops = static_cast<S*>(h->pops[h->cur]);
-  for (int i = 0; i < Q; ++i) {
-    char* hp = static_cast<char*>(host) + i * N * hb;
-    void* dev = direct ? static_cast<void*>(pops + i * L.dstride) : h->stage;
-    if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, hp, L.nx * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      if (!direct)
-        k_pops_in<S, R, H><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-            L, static_cast<const H*>(h->stage), pops + i * L.dstride, h->sp.shift[i], h->sp.scale);
-    } else {
-      if (!direct)
-        k_pops_out<S, R, H><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-            L, static_cast<H*>(h->stage), pops + i * L.dstride, h->sp.shift[i],
-            h->sp.inv_scale);
-      FLB_CUDA(cudaMemcpy2DAsync(hp, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
-    }
-    FLB_CUDA(cudaGetLastError());
+  const long long gn = (long long)gx * gy * gz;
+  if (gn > (1LL << 33)) return fail(FLB_ERR_INVALID, "global block extent too large");
+  std::vector<int> owner(size_t(gn), -1);
+  for (int k = 0; k < nb; ++k) {
+    const HostBlock& b = h->blocks[k];
+    for (int z = b.oz + 1; z < b.oz + b.L.nz - 1; ++z)
+      for (int y = b.oy + 1; y < b.oy + b.L.ny - 1; ++y)
+        for (int x = b.ox + 1; x < b.ox + b.L.nx - 1; ++x) {
+          int& o = owner[size_t((long long)(z * (long long)gy + y) * gx + x)];
+          if (o >= 0) return fail(FLB_ERR_INVALID, "blocks %d and %d overlap in their interiors", o, k);
+          o = k;
+        }
   }
-  FLB_CUDA(cudaStreamSynchronize(st));
-  return FLB_OK;
-}
-
-template <typename S, typename R>
-int pops_transfer_any(flb_lattice* h, void* host, int host_dtype, bool upload, cudaStream_t st) {
-  if (host_dtype == FLB_DTYPE_F32) return pops_transfer<S, R, float>(h, host, upload, st);
-  if (host_dtype == FLB_DTYPE_F64) return pops_transfer<S, R, double>(h, host, upload, st);
-  return fail(FLB_ERR_INVALID, "bad host dtype %d", host_dtype);
-}
-
-template <typename R, typename H>
-int field_transfer(flb_lattice* h, int field, void* host, bool upload, cudaStream_t st) {
-  const LayoutParams& L = h->L;
-  const size_t hb = sizeof(H);
-  if (field == FLB_FIELD_RHO) {
-    const bool direct = std::is_same<R, H>::value;
-    if (!direct) {
-      int rc = ensure_stage(h, size_t(L.dstride) * sizeof(H));
-      if (rc) return rc;
-    }
-    void* dev = direct ? h->rho : h->stage;
-    if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, host, L.nx * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      if (!direct)
-        k_convert<H, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-            L.plane * L.nz, static_cast<const H*>(h->stage), static_cast<R*>(h->rho));
-    } else {
-      if (!direct)
-        k_convert<R, H><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-            L.plane * L.nz, static_cast<const R*>(h->rho), static_cast<H*>(h->stage));
-      FLB_CUDA(cudaMemcpy2DAsync(host, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
-    }
-  } else if (field == FLB_FIELD_VELOCITY) {
-    int rc = ensure_stage(h, 3 * size_t(L.dstride) * sizeof(H));
-    if (rc) return rc;
-    if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(h->stage, 3 * L.pitch * hb, host, 3 * L.nx * hb, 3 * L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      k_vel_in<R, H><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-          L, static_cast<const H*>(h->stage), static_cast<R*>(h->vel));
-    } else {
-      k_vel_out<R, H><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-          L, static_cast<H*>(h->stage), static_cast<const R*>(h->vel));
-      FLB_CUDA(cudaMemcpy2DAsync(host, 3 * L.nx * hb, h->stage, 3 * L.pitch * hb, 3 * L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
-    }
-  } else {
-    return fail(FLB_ERR_INVALID, "unknown field %d", field);
+  std::vector<HaloRec> recs;
+  for (int k = 0; k < nb; ++k) {
+    const HostBlock& b = h->blocks[k];
+    for (int lz = 0; lz < b.L.nz; ++lz)
+      for (int ly = 0; ly < b.L.ny; ++ly)
+        for (int lx = 0; lx < b.L.nx; ++lx) {
+          const bool inner = lx > 0 && ly > 0 && lz > 0 && lx < b.L.nx - 1 && ly < b.L.ny - 1 &&
+                             lz < b.L.nz - 1;
+          if (inner) continue;
+          const int x = b.ox + lx, y = b.oy + ly, z = b.oz + lz;
+          const int o = owner[size_t((long long)(z * (long long)gy + y) * gx + x)];
+          if (o < 0) continue;
+          const HostBlock& n = h->blocks[o];
+          unsigned mask = 0;
+          for (int i = 1; i < Q; ++i) {
+            const int c[3] = {cx(i), cy(i), cz(i)};
+            const int l[3] = {lx, ly, lz};
+            const int m[3] = {b.L.nx, b.L.ny, b.L.nz};
+            for (int a = 0; a < 3; ++a) {
+              if ((l[a] == 0 && c[a] > 0) || (l[a] == m[a] - 1 && c[a] < 0)) mask |= 1u << i;
+            }
+          }
+          HaloRec r;
+          r.dst = b.base + lx + (long long)ly * b.L.pitch + (long long)lz * b.L.plane;
+          const int nx_ = x - n.ox, ny_ = y - n.oy, nz_ = z - n.oz;
+          r.src = n.base + nx_ + (long long)ny_ * n.L.pitch + (long long)nz_ * n.L.plane;
+          r.mask = mask;
+          recs.push_back(r);
+        }
   }
-  FLB_CUDA(cudaGetLastError());
-  FLB_CUDA(cudaStreamSynchronize(st));
+  h->nhalo = (long long)recs.size();
+  if (!recs.empty()) {
+    FLB_CUDA(cudaMalloc((void**)&h->d_halo, recs.size() * sizeof(HaloRec)));
+    FLB_CUDA(cudaMemcpy(h->d_halo, recs.data(), recs.size() * sizeof(HaloRec),
+                        cudaMemcpyHostToDevice));
+  }
   return FLB_OK;
 }
 
@@ -267,6 +288,254 @@ int with_types(flb_lattice* h, F&& f) {
     case FLB_STORAGE_FP16S: return f((__half*)nullptr, (float*)nullptr);
     default: return f((double*)nullptr, (double*)nullptr);
   }
+}
+
+template <typename S, typename R, int MODEL>
+void launch_one_step(flb_lattice* h, cudaStream_t st) {
+  const bool single = h->mode < 0 && h->ctas_per_sm == 0;
+  const dim3 block(32, h->tile_y);
+  if (single) {
+    const HostBlock& b = h->blocks[0];
+    const dim3 grid(b.L.pitch / 32, (b.L.ny + h->tile_y - 1) / h->tile_y, b.L.nz);
+    k_stream_collide<S, R, MODEL><<<grid, block, 0, st>>>(h->sp);
+  } else {
+    long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
+    g = std::max(1LL, std::min(g, h->ntiles));
+    k_stream_collide_blocks<S, R, MODEL><<<unsigned(g), block, 0, st>>>(
+        h->sp, h->d_blocks, int(h->blocks.size()), h->ntiles);
+  }
+  if (h->nhalo > 0)
+    k_halo<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, int(h->nhalo),
+                                                 static_cast<S*>(h->sp.dst), h->dstride);
+}
+
+template <typename S, typename R>
+int launch_steps(flb_lattice* h, int nsteps, cudaStream_t st) {
+  if (h->mode >= 0 || h->ctas_per_sm > 0) FLB_TRY(upload_block_table(h));
+  for (int s = 0; s < nsteps; ++s) {
+    h->sp.src = h->pops[h->cur];
+    h->sp.dst = h->pops[h->cur ^ 1];
+    switch (h->desc.model) {
+      case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
+      case FLB_MODEL_MRT: launch_one_step<S, R, MODEL_MRT>(h, st); break;
+      default: launch_one_step<S, R, MODEL_LES>(h, st); break;
+    }
+    h->cur ^= 1;
+  }
+  FLB_CUDA(cudaGetLastError());
+  return FLB_OK;
+}
+
+int step_any(flb_lattice* h, int nsteps, cudaStream_t st) {
+  return with_types(h, [&](auto* sp, auto* rp) {
+    using S = std::remove_pointer_t<decltype(sp)>;
+    using R = std::remove_pointer_t<decltype(rp)>;
+    return launch_steps<S, R>(h, nsteps, st);
+  });
+}
+
+int check_block(flb_lattice* h, int b) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (b < 0 || b >= int(h->blocks.size()))
+    return fail(FLB_ERR_INVALID, "block %d outside [0, %zu)", b, h->blocks.size());
+  return FLB_OK;
+}
+
+template <typename S, typename R, typename H>
+int pops_transfer(flb_lattice* h, const HostBlock& B, void* host, bool upload, cudaStream_t st) {
+  const LayoutParams& L = B.L;
+  const size_t hb = sizeof(H);
+  const size_t N = size_t(L.nx) * L.ny * L.nz;
+  const bool direct = std::is_same<S, H>::value;
+  if (!direct) FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
+  S* pops = static_cast<S*>(h->pops[h->cur]) + B.base;
+  for (int i = 0; i < Q; ++i) {
+    char* hp = static_cast<char*>(host) + i * N * hb;
+    void* dev = direct ? static_cast<void*>(pops + i * h->dstride) : h->stage;
+    if (upload) {
+      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, hp, L.nx * hb, L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
+      if (!direct)
+        k_pops_in<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
+            L, static_cast<const H*>(h->stage), pops + i * h->dstride, h->sp.shift[i],
+            h->sp.scale);
+    } else {
+      if (!direct)
+        k_pops_out<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
+            L, static_cast<H*>(h->stage), pops + i * h->dstride, h->sp.shift[i],
+            h->sp.inv_scale);
+      FLB_CUDA(cudaMemcpy2DAsync(hp, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+    }
+    FLB_CUDA(cudaGetLastError());
+  }
+  FLB_CUDA(cudaStreamSynchronize(st));
+  return FLB_OK;
+}
+
+int pops_any(flb_lattice* h, int b, void* host, int host_dtype, bool upload, void* stream) {
+  FLB_TRY(check_block(h, b));
+  if (!host) return fail(FLB_ERR_INVALID, "null host buffer");
+  if (host_dtype != FLB_DTYPE_F32 && host_dtype != FLB_DTYPE_F64)
+    return fail(FLB_ERR_INVALID, "bad host dtype %d", host_dtype);
+  const HostBlock& B = h->blocks[b];
+  cudaStream_t st = as_stream(stream);
+  return with_types(h, [&](auto* sp, auto* rp) {
+    using S = std::remove_pointer_t<decltype(sp)>;
+    using R = std::remove_pointer_t<decltype(rp)>;
+    if (host_dtype == FLB_DTYPE_F32) return pops_transfer<S, R, float>(h, B, host, upload, st);
+    return pops_transfer<S, R, double>(h, B, host, upload, st);
+  });
+}
+
+template <typename R, typename H>
+int field_transfer(flb_lattice* h, const HostBlock& B, int field, void* host, bool upload,
+                   cudaStream_t st) {
+  const LayoutParams& L = B.L;
+  const size_t hb = sizeof(H);
+  R* rho = static_cast<R*>(h->rho) + B.base;
+  R* vel = static_cast<R*>(h->vel) + B.base;
+  if (field == FLB_FIELD_RHO) {
+    const bool direct = std::is_same<R, H>::value;
+    if (!direct) FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
+    void* dev = direct ? static_cast<void*>(rho) : h->stage;
+    if (upload) {
+      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, host, L.nx * hb, L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
+      if (!direct)
+        k_convert<H, R><<<grid_1d(B.padded()), 256, 0, st>>>(
+            B.padded(), static_cast<const H*>(h->stage), rho);
+    } else {
+      if (!direct)
+        k_convert<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(B.padded(), rho,
+                                                             static_cast<H*>(h->stage));
+      FLB_CUDA(cudaMemcpy2DAsync(host, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+    }
+  } else if (field == FLB_FIELD_VELOCITY) {
+    FLB_TRY(ensure_stage(h, 3 * size_t(B.padded()) * sizeof(H)));
+    if (upload) {
+      FLB_CUDA(cudaMemcpy2DAsync(h->stage, 3 * L.pitch * hb, host, 3 * L.nx * hb, 3 * L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
+      k_vel_in<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(L, static_cast<const H*>(h->stage),
+                                                          vel);
+    } else {
+      k_vel_out<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(L, static_cast<H*>(h->stage), vel);
+      FLB_CUDA(cudaMemcpy2DAsync(host, 3 * L.nx * hb, h->stage, 3 * L.pitch * hb, 3 * L.nx * hb,
+                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+    }
+  } else {
+    return fail(FLB_ERR_INVALID, "unknown field %d", field);
+  }
+  FLB_CUDA(cudaGetLastError());
+  FLB_CUDA(cudaStreamSynchronize(st));
+  return FLB_OK;
+}
+
+int field_any(flb_lattice* h, int b, int field, void* host, int host_dtype, bool upload,
+              void* stream) {
+  FLB_TRY(check_block(h, b));
+  if (!host) return fail(FLB_ERR_INVALID, "null host buffer");
+  const HostBlock& B = h->blocks[b];
+  cudaStream_t st = as_stream(stream);
+  if (h->real_bytes == 8) {
+    if (host_dtype == FLB_DTYPE_F64) return field_transfer<double, double>(h, B, field, host, upload, st);
+    if (host_dtype == FLB_DTYPE_F32) return field_transfer<double, float>(h, B, field, host, upload, st);
+  } else {
+    if (host_dtype == FLB_DTYPE_F64) return field_transfer<float, double>(h, B, field, host, upload, st);
+    if (host_dtype == FLB_DTYPE_F32) return field_transfer<float, float>(h, B, field, host, upload, st);
+  }
+  return fail(FLB_ERR_INVALID, "bad host dtype %d", host_dtype);
+}
+
+int flags_any(flb_lattice* h, int b, uint8_t* host, bool upload, void* stream) {
+  FLB_TRY(check_block(h, b));
+  if (!host) return fail(FLB_ERR_INVALID, "null host buffer");
+  const HostBlock& B = h->blocks[b];
+  const LayoutParams& L = B.L;
+  cudaStream_t st = as_stream(stream);
+  if (upload)
+    FLB_CUDA(cudaMemcpy2DAsync(h->flags + B.base, L.pitch, host, L.nx, L.nx,
+                               size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
+  else
+    FLB_CUDA(cudaMemcpy2DAsync(host, L.nx, h->flags + B.base, L.pitch, L.nx,
+                               size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+  FLB_CUDA(cudaStreamSynchronize(st));
+  return FLB_OK;
+}
+
+// Common allocation for flb_create / flb_create_blocks.
+int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, int mode,
+                  flb_lattice** out) {
+  flb_lattice* h = new (std::nothrow) flb_lattice();
+  if (!h) return fail(FLB_ERR_OOM, "host allocation failed");
+  auto cleanup = [&](int code) {
+    flb_destroy(h);
+    return code;
+  };
+  h->desc = *desc;
+  h->mode = mode;
+  cudaGetDevice(&h->device);
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device) == cudaSuccess &&
+      sms > 0)
+    h->sm_count = sms;
+  h->elem_bytes =
+      desc->storage == FLB_STORAGE_FP16S ? 2 : (desc->storage == FLB_STORAGE_FP64 ? 8 : 4);
+  h->real_bytes = desc->storage == FLB_STORAGE_FP64 ? 8 : 4;
+  long long off = 0;
+  for (HostBlock& b : blocks) {
+    b.L.pitch = (b.L.nx + 31) / 32 * 32;
+    b.L.plane = (long long)b.L.pitch * b.L.ny;
+    b.base = off;
+    off += (b.padded() + 63) / 64 * 64;
+  }
+  h->dstride = off;
+  for (HostBlock& b : blocks) b.L.dstride = h->dstride;
+  h->blocks = std::move(blocks);
+  const size_t ds = size_t(h->dstride);
+  const size_t popb = size_t(Q) * ds * h->elem_bytes;
+  cudaError_t e;
+  for (int k = 0; k < 2; ++k)
+    if ((e = cudaMalloc(&h->pops[k], popb)) != cudaSuccess)
+      return cleanup(fail(FLB_ERR_OOM, "cudaMalloc populations (%zu bytes): %s", popb,
+                          cudaGetErrorString(e)));
+  if ((e = cudaMalloc((void**)&h->flags, ds)) != cudaSuccess ||
+      (e = cudaMalloc(&h->rho, ds * h->real_bytes)) != cudaSuccess ||
+      (e = cudaMalloc(&h->vel, 3 * ds * h->real_bytes)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess)
+    return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
+  build_params(h);
+  if (mode == FLB_BLOCKS_HALO) {
+    int rc = build_halo(h);
+    if (rc) return cleanup(rc);
+  }
+  cudaStream_t st = 0;
+  if ((e = cudaMemsetAsync(h->flags, 1, ds, st)) != cudaSuccess ||
+      (e = cudaMemsetAsync(h->vel, 0, 3 * ds * h->real_bytes, st)) != cudaSuccess)
+    return cleanup(fail(FLB_ERR_CUDA, "init memset: %s", cudaGetErrorString(e)));
+  if (h->real_bytes == 8)
+    k_fill<double><<<grid_1d(ds), 256, 0, st>>>(h->dstride, static_cast<double*>(h->rho),
+                                                 desc->rho0);
+  else
+    k_fill<float><<<grid_1d(ds), 256, 0, st>>>(h->dstride, static_cast<float*>(h->rho),
+                                                float(desc->rho0));
+  int rc = flb_init_equilibrium(h, desc->rho0, nullptr);
+  if (rc) return cleanup(rc);
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cleanup(fail(FLB_ERR_CUDA, "create: %s", cudaGetErrorString(e)));
+  *out = h;
+  return FLB_OK;
+}
+
+// Run a per-block helper kernel over every block.
+template <typename F>
+int for_blocks(flb_lattice* h, F&& f) {
+  for (const HostBlock& b : h->blocks) {
+    int rc = f(b);
+    if (rc) return rc;
+  }
+  return FLB_OK;
 }
 
 }  // namespace
@@ -307,151 +576,126 @@ int flb_desc_default(flb_lattice_desc* d, int nx, int ny, int nz, double tau) {
 int flb_create(const flb_lattice_desc* desc, flb_lattice** out) {
   if (!out) return fail(FLB_ERR_INVALID, "null output handle");
   *out = nullptr;
-  int rc = validate_desc(desc);
-  if (rc) return rc;
-  flb_lattice* h = new (std::nothrow) flb_lattice();
-  if (!h) return fail(FLB_ERR_OOM, "host allocation failed");
-  h->desc = *desc;
-  cudaGetDevice(&h->device);
-  const int elem =
-      desc->storage == FLB_STORAGE_FP16S ? 2 : (desc->storage == FLB_STORAGE_FP64 ? 8 : 4);
-  const int real = desc->storage == FLB_STORAGE_FP64 ? 8 : 4;
-  h->elem_bytes = elem;
-  h->real_bytes = real;
-  LayoutParams& L = h->L;
-  L.nx = desc->nx;
-  L.ny = desc->ny;
-  L.nz = desc->nz;
-  L.pitch = (desc->nx + 31) / 32 * 32;
-  L.plane = (long long)L.pitch * L.ny;
-  L.dstride = (L.plane * L.nz + 63) / 64 * 64;
-  const size_t popb = size_t(Q) * L.dstride * elem;
-  auto cleanup = [&](int code) {
-    flb_destroy(h);
-    return code;
-  };
-  cudaError_t e;
-  for (int b = 0; b < 2; ++b) {
-    e = cudaMalloc(&h->pops[b], popb);
-    if (e != cudaSuccess)
-      return cleanup(fail(FLB_ERR_OOM, "cudaMalloc populations (%zu bytes): %s", popb,
-                          cudaGetErrorString(e)));
+  FLB_TRY(validate_common(desc));
+  FLB_TRY(validate_block(desc->nx, desc->ny, desc->nz));
+  HostBlock b{};
+  b.L.nx = desc->nx;
+  b.L.ny = desc->ny;
+  b.L.nz = desc->nz;
+  b.omega = arith_omega(*desc, desc->omega);
+  return create_common(desc, {b}, -1, out);
+}
+
+int flb_create_blocks(const flb_lattice_desc* desc, int nblocks, const flb_block_desc* blocks,
+                      int mode, flb_lattice** out) {
+  if (!out) return fail(FLB_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  FLB_TRY(validate_common(desc));
+  if (nblocks < 1 || !blocks) return fail(FLB_ERR_INVALID, "need at least one block");
+  if (mode != FLB_BLOCKS_INDEPENDENT && mode != FLB_BLOCKS_HALO)
+    return fail(FLB_ERR_INVALID, "bad multi-block mode %d", mode);
+  std::vector<HostBlock> v(nblocks);
+  for (int k = 0; k < nblocks; ++k) {
+    const flb_block_desc& d = blocks[k];
+    FLB_TRY(validate_block(d.nx, d.ny, d.nz));
+    const double om = d.omega > 0.0 ? d.omega : desc->omega;
+    if (!(om > 0.0 && om < 2.0)) return fail(FLB_ERR_INVALID, "block %d omega %g", k, om);
+    v[k] = HostBlock{};
+    v[k].L.nx = d.nx;
+    v[k].L.ny = d.ny;
+    v[k].L.nz = d.nz;
+    v[k].ox = d.ox;
+    v[k].oy = d.oy;
+    v[k].oz = d.oz;
+    v[k].omega = arith_omega(*desc, om);
   }
-  if ((e = cudaMalloc((void**)&h->flags, size_t(L.dstride))) != cudaSuccess ||
-      (e = cudaMalloc(&h->rho, size_t(L.dstride) * real)) != cudaSuccess ||
-      (e = cudaMalloc(&h->vel, 3 * size_t(L.dstride) * real)) != cudaSuccess ||
-      (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess)
-    return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
-  build_params(h);
-  // defaults: void flags, RHO = rho0, VELOCITY = 0, f = rho0 * w_i
-  cudaStream_t st = 0;
-  if ((e = cudaMemsetAsync(h->flags, 1, size_t(L.dstride), st)) != cudaSuccess ||
-      (e = cudaMemsetAsync(h->vel, 0, 3 * size_t(L.dstride) * real, st)) != cudaSuccess)
-    return cleanup(fail(FLB_ERR_CUDA, "init memset: %s", cudaGetErrorString(e)));
-  if (real == 8)
-    k_fill<double><<<grid_1d(L.dstride), 256, 0, st>>>(L.dstride, static_cast<double*>(h->rho),
-                                                        desc->rho0);
-  else
-    k_fill<float><<<grid_1d(L.dstride), 256, 0, st>>>(L.dstride, static_cast<float*>(h->rho),
-                                                       float(desc->rho0));
-  rc = flb_init_equilibrium(h, desc->rho0, nullptr);
-  if (rc) return cleanup(rc);
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return cleanup(fail(FLB_ERR_CUDA, "create: %s", cudaGetErrorString(e)));
-  *out = h;
-  return FLB_OK;
+  return create_common(desc, std::move(v), mode, out);
 }
 
 int flb_destroy(flb_lattice* h) {
   if (!h) return FLB_OK;
+  drop_graphs(h);
   for (void* p : {h->pops[0], h->pops[1], (void*)h->flags, h->rho, h->vel, (void*)h->acc,
-                  h->stage, (void*)h->uprev})
+                  h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo})
     if (p) cudaFree(p);
   delete h;
   return FLB_OK;
 }
 
+int flb_block_count(const flb_lattice* h, int* n) {
+  if (!h || !n) return fail(FLB_ERR_INVALID, "null argument");
+  *n = int(h->blocks.size());
+  return FLB_OK;
+}
+
+int flb_halo_count(const flb_lattice* h, long long* n) {
+  if (!h || !n) return fail(FLB_ERR_INVALID, "null argument");
+  *n = h->nhalo;
+  return FLB_OK;
+}
+
 int flb_memory_bytes(const flb_lattice* h, size_t* bytes) {
   if (!h || !bytes) return fail(FLB_ERR_INVALID, "null argument");
-  const size_t ds = size_t(h->L.dstride);
+  const size_t ds = size_t(h->dstride);
   *bytes = 2 * size_t(Q) * ds * h->elem_bytes + ds + 4 * ds * h->real_bytes + 64 +
-           h->stage_bytes + (h->uprev ? 3 * ds * sizeof(double) : 0);
+           h->stage_bytes + (h->uprev ? 3 * ds * sizeof(double) : 0) +
+           h->blocks.size() * sizeof(BlockEntry) + size_t(h->nhalo) * sizeof(HaloRec);
   return FLB_OK;
 }
 
 int flb_upload_flags(flb_lattice* h, const uint8_t* host, void* stream) {
-  if (!h || !host) return fail(FLB_ERR_INVALID, "null argument");
-  const LayoutParams& L = h->L;
-  cudaStream_t st = as_stream(stream);
-  FLB_CUDA(cudaMemcpy2DAsync(h->flags, L.pitch, host, L.nx, L.nx, size_t(L.ny) * L.nz,
-                             cudaMemcpyHostToDevice, st));
-  FLB_CUDA(cudaStreamSynchronize(st));
-  return FLB_OK;
+  return flags_any(h, 0, const_cast<uint8_t*>(host), true, stream);
 }
-
 int flb_download_flags(flb_lattice* h, uint8_t* host, void* stream) {
-  if (!h || !host) return fail(FLB_ERR_INVALID, "null argument");
-  const LayoutParams& L = h->L;
-  cudaStream_t st = as_stream(stream);
-  FLB_CUDA(cudaMemcpy2DAsync(host, L.nx, h->flags, L.pitch, L.nx, size_t(L.ny) * L.nz,
-                             cudaMemcpyDeviceToHost, st));
-  FLB_CUDA(cudaStreamSynchronize(st));
-  return FLB_OK;
+  return flags_any(h, 0, host, false, stream);
+}
+int flb_upload_flags_block(flb_lattice* h, int b, const uint8_t* host, void* stream) {
+  return flags_any(h, b, const_cast<uint8_t*>(host), true, stream);
+}
+int flb_download_flags_block(flb_lattice* h, int b, uint8_t* host, void* stream) {
+  return flags_any(h, b, host, false, stream);
 }
 
-int flb_upload_pops(flb_lattice* h, const void* host, int host_dtype, void* stream) {
-  if (!h || !host) return fail(FLB_ERR_INVALID, "null argument");
-  return with_types(h, [&](auto* sp, auto* rp) {
-    using S = std::remove_pointer_t<decltype(sp)>;
-    using R = std::remove_pointer_t<decltype(rp)>;
-    return pops_transfer_any<S, R>(h, const_cast<void*>(host), host_dtype, true,
-                                   as_stream(stream));
-  });
+int flb_upload_pops(flb_lattice* h, const void* host, int dt, void* stream) {
+  return pops_any(h, 0, const_cast<void*>(host), dt, true, stream);
+}
+int flb_download_pops(flb_lattice* h, void* host, int dt, void* stream) {
+  return pops_any(h, 0, host, dt, false, stream);
+}
+int flb_upload_pops_block(flb_lattice* h, int b, const void* host, int dt, void* stream) {
+  return pops_any(h, b, const_cast<void*>(host), dt, true, stream);
+}
+int flb_download_pops_block(flb_lattice* h, int b, void* host, int dt, void* stream) {
+  return pops_any(h, b, host, dt, false, stream);
 }
 
-int flb_download_pops(flb_lattice* h, void* host, int host_dtype, void* stream) {
-  if (!h || !host) return fail(FLB_ERR_INVALID, "null argument");
-  return with_types(h, [&](auto* sp, auto* rp) {
-    using S = std::remove_pointer_t<decltype(sp)>;
-    using R = std::remove_pointer_t<decltype(rp)>;
-    return pops_transfer_any<S, R>(h, host, host_dtype, false, as_stream(stream));
-  });
+int flb_upload_field(flb_lattice* h, int field, const void* host, int dt, void* stream) {
+  return field_any(h, 0, field, const_cast<void*>(host), dt, true, stream);
 }
-
-static int field_any(flb_lattice* h, int field, void* host, int host_dtype, bool upload,
-                     void* stream) {
-  if (!h || !host) return fail(FLB_ERR_INVALID, "null argument");
-  cudaStream_t st = as_stream(stream);
-  if (h->real_bytes == 8) {
-    if (host_dtype == FLB_DTYPE_F64) return field_transfer<double, double>(h, field, host, upload, st);
-    if (host_dtype == FLB_DTYPE_F32) return field_transfer<double, float>(h, field, host, upload, st);
-  } else {
-    if (host_dtype == FLB_DTYPE_F64) return field_transfer<float, double>(h, field, host, upload, st);
-    if (host_dtype == FLB_DTYPE_F32) return field_transfer<float, float>(h, field, host, upload, st);
-  }
-  return fail(FLB_ERR_INVALID, "bad host dtype %d", host_dtype);
+int flb_download_field(flb_lattice* h, int field, void* host, int dt, void* stream) {
+  return field_any(h, 0, field, host, dt, false, stream);
 }
-
-int flb_upload_field(flb_lattice* h, int field, const void* host, int host_dtype, void* stream) {
-  return field_any(h, field, const_cast<void*>(host), host_dtype, true, stream);
+int flb_upload_field_block(flb_lattice* h, int b, int field, const void* host, int dt,
+                           void* stream) {
+  return field_any(h, b, field, const_cast<void*>(host), dt, true, stream);
 }
-
-int flb_download_field(flb_lattice* h, int field, void* host, int host_dtype, void* stream) {
-  return field_any(h, field, host, host_dtype, false, stream);
+int flb_download_field_block(flb_lattice* h, int b, int field, void* host, int dt,
+                             void* stream) {
+  return field_any(h, b, field, host, dt, false, stream);
 }
 
 int flb_init_equilibrium(flb_lattice* h, double rho0, void* stream) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   cudaStream_t st = as_stream(stream);
-  const LayoutParams& L = h->L;
-  int rc = with_types(h, [&](auto* sp, auto* rp) {
+  FLB_TRY(with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    k_init_equilibrium<S, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-        L, static_cast<S*>(h->pops[h->cur]), rho0, h->sp);
-    return FLB_OK;
-  });
-  if (rc) return rc;
+    return for_blocks(h, [&](const HostBlock& b) {
+      k_init_equilibrium<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, static_cast<S*>(h->pops[h->cur]) + b.base, rho0, h->sp);
+      return FLB_OK;
+    });
+  }));
   FLB_CUDA(cudaGetLastError());
   return FLB_OK;
 }
@@ -460,27 +704,120 @@ int flb_step(flb_lattice* h, int nsteps, void* stream) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   if (nsteps < 0) return fail(FLB_ERR_INVALID, "nsteps %d < 0", nsteps);
   if (nsteps == 0) return FLB_OK;
+  return step_any(h, nsteps, as_stream(stream));
+}
+
+int flb_step_graph(flb_lattice* h, int nsteps, void* stream) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (nsteps < 0) return fail(FLB_ERR_INVALID, "nsteps %d < 0", nsteps);
   cudaStream_t st = as_stream(stream);
-  return with_types(h, [&](auto* sp, auto* rp) {
-    using S = std::remove_pointer_t<decltype(sp)>;
-    using R = std::remove_pointer_t<decltype(rp)>;
-    return launch_step_t<S, R>(h, nsteps, st);
-  });
+  const int pairs = nsteps / 2;
+  if (pairs > 0) {
+    const int parity = h->cur;
+    if (!h->graph[parity]) {
+      if (h->mode >= 0 || h->ctas_per_sm > 0) FLB_TRY(upload_block_table(h));
+      cudaStream_t cap;
+      FLB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      cudaGraph_t graph = nullptr;
+      cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+      int rc = FLB_OK;
+      if (e == cudaSuccess) {
+        rc = step_any(h, 2, cap);  // advances h->cur by two: parity unchanged
+        e = cudaStreamEndCapture(cap, &graph);
+      }
+      cudaStreamDestroy(cap);
+      if (rc) return rc;
+      if (e != cudaSuccess) return fail(FLB_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&h->graph[parity], graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess)
+        return fail(FLB_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    for (int k = 0; k < pairs; ++k) FLB_CUDA(cudaGraphLaunch(h->graph[parity], st));
+  }
+  if (nsteps & 1) return step_any(h, 1, st);
+  return FLB_OK;
+}
+
+int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (tile_y != 1 && tile_y != 2 && tile_y != 4 && tile_y != 8)
+    return fail(FLB_ERR_INVALID, "tile_y %d not in {1,2,4,8}", tile_y);
+  if (ctas_per_sm < 0 || ctas_per_sm > 32)
+    return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [0, 32]", ctas_per_sm);
+  if (tile_y != h->tile_y || ctas_per_sm != h->ctas_per_sm) drop_graphs(h);
+  h->tile_y = tile_y;
+  h->ctas_per_sm = ctas_per_sm;
+  return FLB_OK;
+}
+
+int flb_get_launch(const flb_lattice* h, int* tile_y, int* ctas_per_sm) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (tile_y) *tile_y = h->tile_y;
+  if (ctas_per_sm) *ctas_per_sm = h->ctas_per_sm;
+  return FLB_OK;
+}
+
+int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int* ctas_per_sm,
+                 double* best_ms, int* steps_taken) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (trial_steps < 1) return fail(FLB_ERR_INVALID, "trial_steps %d < 1", trial_steps);
+  cudaStream_t st = as_stream(stream);
+  const int tys[] = {1, 2, 4, 8};
+  const int ctas[] = {0, 2, 4, 8};
+  const int ty0 = h->tile_y, c0 = h->ctas_per_sm;
+  int best_ty = ty0, best_c = c0, taken = 0;
+  float best = 1e30f;
+  cudaEvent_t e0, e1;
+  FLB_CUDA(cudaEventCreate(&e0));
+  FLB_CUDA(cudaEventCreate(&e1));
+  int rc = FLB_OK;
+  for (int ty : tys) {
+    for (int c : ctas) {
+      if ((rc = flb_set_launch(h, ty, c))) break;
+      if ((rc = step_any(h, 1, st))) break;  // warm-up (block table upload, caches)
+      cudaEventRecord(e0, st);
+      if ((rc = step_any(h, trial_steps, st))) break;
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      taken += trial_steps + 1;
+      if (ms < best) {
+        best = ms;
+        best_ty = ty;
+        best_c = c;
+      }
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    flb_set_launch(h, ty0, c0);
+    return rc;
+  }
+  FLB_TRY(flb_set_launch(h, best_ty, best_c));
+  if (tile_y) *tile_y = best_ty;
+  if (ctas_per_sm) *ctas_per_sm = best_c;
+  if (best_ms) *best_ms = double(best) / trial_steps;
+  if (steps_taken) *steps_taken = taken;
+  return FLB_OK;
 }
 
 int flb_compute_rhou(flb_lattice* h, uint8_t key, void* stream) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   cudaStream_t st = as_stream(stream);
-  const LayoutParams& L = h->L;
-  int rc = with_types(h, [&](auto* sp, auto* rp) {
+  FLB_TRY(with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    k_rhou<S, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-        L, static_cast<const S*>(h->pops[h->cur]), h->flags, key, static_cast<R*>(h->rho),
-        static_cast<R*>(h->vel), h->sp);
-    return FLB_OK;
-  });
-  if (rc) return rc;
+    return for_blocks(h, [&](const HostBlock& b) {
+      k_rhou<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key,
+          static_cast<R*>(h->rho) + b.base, static_cast<R*>(h->vel) + b.base, h->sp);
+      return FLB_OK;
+    });
+  }));
   FLB_CUDA(cudaGetLastError());
   return FLB_OK;
 }
@@ -488,16 +825,17 @@ int flb_compute_rhou(flb_lattice* h, uint8_t key, void* stream) {
 int flb_reduce_conservation(flb_lattice* h, uint8_t key, double out[4], void* stream) {
   if (!h || !out) return fail(FLB_ERR_INVALID, "null argument");
   cudaStream_t st = as_stream(stream);
-  const LayoutParams& L = h->L;
   FLB_CUDA(cudaMemsetAsync(h->acc, 0, 4 * sizeof(double), st));
-  int rc = with_types(h, [&](auto* sp, auto* rp) {
+  FLB_TRY(with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    k_conservation<S, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-        L, static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->acc, h->sp);
-    return FLB_OK;
-  });
-  if (rc) return rc;
+    return for_blocks(h, [&](const HostBlock& b) {
+      k_conservation<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key, h->acc,
+          h->sp);
+      return FLB_OK;
+    });
+  }));
   FLB_CUDA(cudaGetLastError());
   FLB_CUDA(cudaMemcpyAsync(out, h->acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   FLB_CUDA(cudaStreamSynchronize(st));
@@ -507,21 +845,22 @@ int flb_reduce_conservation(flb_lattice* h, uint8_t key, double out[4], void* st
 int flb_tolerance_u(flb_lattice* h, uint8_t key, double* max_du, void* stream) {
   if (!h || !max_du) return fail(FLB_ERR_INVALID, "null argument");
   cudaStream_t st = as_stream(stream);
-  const LayoutParams& L = h->L;
   if (!h->uprev) {
-    FLB_CUDA(cudaMalloc((void**)&h->uprev, 3 * size_t(L.dstride) * sizeof(double)));
-    FLB_CUDA(cudaMemsetAsync(h->uprev, 0, 3 * size_t(L.dstride) * sizeof(double), st));
+    FLB_CUDA(cudaMalloc((void**)&h->uprev, 3 * size_t(h->dstride) * sizeof(double)));
+    FLB_CUDA(cudaMemsetAsync(h->uprev, 0, 3 * size_t(h->dstride) * sizeof(double), st));
   }
   unsigned long long* acc = reinterpret_cast<unsigned long long*>(h->acc);
   FLB_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), st));
-  int rc = with_types(h, [&](auto* sp, auto* rp) {
+  FLB_TRY(with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    k_tolerance<S, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-        L, static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->uprev, acc, h->sp);
-    return FLB_OK;
-  });
-  if (rc) return rc;
+    return for_blocks(h, [&](const HostBlock& b) {
+      k_tolerance<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key,
+          h->uprev + b.base, acc, h->sp);
+      return FLB_OK;
+    });
+  }));
   FLB_CUDA(cudaGetLastError());
   unsigned long long bits = 0;
   FLB_CUDA(cudaMemcpyAsync(&bits, acc, sizeof bits, cudaMemcpyDeviceToHost, st));
@@ -533,17 +872,17 @@ int flb_tolerance_u(flb_lattice* h, uint8_t key, double* max_du, void* stream) {
 int flb_check_finite(flb_lattice* h, uint64_t* bad, void* stream) {
   if (!h || !bad) return fail(FLB_ERR_INVALID, "null argument");
   cudaStream_t st = as_stream(stream);
-  const LayoutParams& L = h->L;
   unsigned long long* acc = reinterpret_cast<unsigned long long*>(h->acc);
   FLB_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long), st));
-  int rc = with_types(h, [&](auto* sp, auto* rp) {
+  FLB_TRY(with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    k_finite<S, R><<<grid_1d(L.plane * L.nz), 256, 0, st>>>(
-        L, static_cast<const S*>(h->pops[h->cur]), acc, h->sp);
-    return FLB_OK;
-  });
-  if (rc) return rc;
+    return for_blocks(h, [&](const HostBlock& b) {
+      k_finite<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, acc, h->sp);
+      return FLB_OK;
+    });
+  }));
   FLB_CUDA(cudaGetLastError());
   unsigned long long v = 0;
   FLB_CUDA(cudaMemcpyAsync(&v, acc, sizeof v, cudaMemcpyDeviceToHost, st));
@@ -554,12 +893,13 @@ int flb_check_finite(flb_lattice* h, uint64_t* bad, void* stream) {
 
 int flb_get_layout(const flb_lattice* h, flb_layout* layout) {
   if (!h || !layout) return fail(FLB_ERR_INVALID, "null argument");
-  layout->nx = h->L.nx;
-  layout->ny = h->L.ny;
-  layout->nz = h->L.nz;
-  layout->pitch_x = h->L.pitch;
-  layout->plane = size_t(h->L.plane);
-  layout->dir_stride = size_t(h->L.dstride);
+  const HostBlock& b = h->blocks[0];
+  layout->nx = b.L.nx;
+  layout->ny = b.L.ny;
+  layout->nz = b.L.nz;
+  layout->pitch_x = b.L.pitch;
+  layout->plane = size_t(b.L.plane);
+  layout->dir_stride = size_t(h->dstride);
   layout->elem_bytes = h->elem_bytes;
   return FLB_OK;
 }

@@ -64,8 +64,8 @@ enum : int { OP_NONE = 0, OP_BULK = 1, OP_BB = 2, OP_MBB = 3, OP_FIELD_BGK = 4 }
 enum : int { MODEL_BGK = 0, MODEL_MRT = 1, MODEL_LES = 2 };
 
 template <typename R, int MODEL>
-__device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long long cell) {
-  const R omega = R(p.omega);
+__device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long long cell,
+                                         R omega) {
   if (op == OP_BULK) {
     if constexpr (MODEL == MODEL_BGK) {
       bgk<R>(f, omega, R(1) - omega);
@@ -74,7 +74,8 @@ __device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long
     } else {
       R s[Q];
 #pragma unroll
-      for (int k = 0; k < Q; ++k) s[k] = R(p.s_over_norm[k]);
+      for (int k = 0; k < Q; ++k)
+        s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm(k))) : R(p.s_over_norm[k]);
       mrt<R>(f, s);
     }
   } else if (op == OP_BB) {
@@ -89,29 +90,32 @@ __device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long
   }
 }
 
-// Destination of population i pushed from an outer-layer cell: the reference
-// linear index wraps modulo ncells (CyclicArray::rotate), then maps back to
-// the padded layout.
-__device__ __forceinline__ long long wrap_dest(const StepParams& p, long long lin, int i) {
-  long long d = lin + p.delta[i];
-  if (d < 0) d += p.ncells;
-  else if (d >= p.ncells) d -= p.ncells;
-  const long long nxy = (long long)p.nx * p.ny;
-  const long long dz = d / nxy;
-  const long long r = d - dz * nxy;
-  const long long dy = r / p.nx;
-  const long long dx = r - dy * p.nx;
-  return dx + dy * p.pitch + dz * p.plane;
+// Geometry of one block inside the population / field arrays.
+struct Geom {
+  int nx, ny, nz, pitch;
+  long long plane;  // pitch * ny
+  long long base;   // element offset of the block's cell (0,0,0)
+};
+
+// Destination of population i pushed from an outer-layer cell.  The reference
+// adds Delta_i = cx + nx*cy + nx*ny*cz to the linear index modulo ncells
+// (CyclicArray::rotate).  With |c| <= 1 per axis that sum is the mixed-radix
+// (nx, ny, nz) addition below: each digit carries at most one unit into the
+// next and the last digit wraps modulo nz, which is the modulo-ncells wrap.
+__device__ __forceinline__ long long wrap_dest(const Geom& g, int x, int y, int z, int i) {
+  int dx = x + cx(i), dy = y + cy(i), dz = z + cz(i);
+  if (dx < 0) { dx += g.nx; --dy; } else if (dx >= g.nx) { dx -= g.nx; ++dy; }
+  if (dy < 0) { dy += g.ny; --dz; } else if (dy >= g.ny) { dy -= g.ny; ++dz; }
+  if (dz < 0) dz += g.nz; else if (dz >= g.nz) dz -= g.nz;
+  return g.base + dx + (long long)dy * g.pitch + (long long)dz * g.plane;
 }
 
-// One fused step: block (32, BY), grid (pitch/32, ceil(ny/BY), nz).
+// One cell of one step: load the 19 populations of (x,y,z), apply the op its
+// flag selects, push population i to the cell Delta_i away in dst.
 template <typename S, typename R, int MODEL>
-__global__ void __launch_bounds__(256) k_stream_collide(const StepParams p) {
-  const int x = blockIdx.x * 32 + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= p.nx || y >= p.ny) return;
-  const long long cell = x + (long long)y * p.pitch + (long long)z * p.plane;
+__device__ __forceinline__ void update_cell(const StepParams& p, const Geom& g, R omega, int x,
+                                            int y, int z) {
+  const long long cell = g.base + x + (long long)y * g.pitch + (long long)z * g.plane;
   const S* __restrict__ src = static_cast<const S*>(p.src);
   S* __restrict__ dst = static_cast<S*>(p.dst);
 
@@ -121,20 +125,84 @@ __global__ void __launch_bounds__(256) k_stream_collide(const StepParams p) {
     f[i] = Storage<S, R>::load(src + i * p.dstride + cell, p.shift[i], p.inv_scale);
 
   const int op = select_op(p, p.flags[cell]);
-  apply_op<R, MODEL>(p, op, f, cell);
+  apply_op<R, MODEL>(p, op, f, cell, omega);
 
   const bool outer =
-      x == 0 || y == 0 || z == 0 || x == p.nx - 1 || y == p.ny - 1 || z == p.nz - 1;
+      x == 0 || y == 0 || z == 0 || x == g.nx - 1 || y == g.ny - 1 || z == g.nz - 1;
   if (!outer) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i)
-      Storage<S, R>::store(dst + i * p.dstride + cell + p.off[i], f[i], p.shift[i], p.scale);
+    for (int i = 0; i < Q; ++i) {
+      const long long off = cx(i) + (long long)cy(i) * g.pitch + (long long)cz(i) * g.plane;
+      Storage<S, R>::store(dst + i * p.dstride + cell + off, f[i], p.shift[i], p.scale);
+    }
   } else {
-    const long long lin = x + (long long)p.nx * (y + (long long)p.ny * z);
 #pragma unroll
     for (int i = 0; i < Q; ++i)
-      Storage<S, R>::store(dst + i * p.dstride + wrap_dest(p, lin, i), f[i], p.shift[i],
+      Storage<S, R>::store(dst + i * p.dstride + wrap_dest(g, x, y, z, i), f[i], p.shift[i],
                            p.scale);
+  }
+}
+
+// Single block: block (32, BY), grid (pitch/32, ceil(ny/BY), nz).
+template <typename S, typename R, int MODEL>
+__global__ void __launch_bounds__(256) k_stream_collide(const StepParams p) {
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= p.nx || y >= p.ny) return;
+  const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
+  update_cell<S, R, MODEL>(p, g, R(p.omega), x, y, z);
+}
+
+// Many blocks in one launch.  Tiles of 32 x blockDim.y cells are numbered
+// block by block (x fastest, then y, then z); tile_start is the first tile of
+// each block.  CTAs walk the tiles with a grid stride, so the grid can be
+// sized to the GPU (persistent) or to the tile count.
+struct BlockEntry {
+  Geom g;
+  double omega;          // per-block 1/tau in the arithmetic type
+  long long tile_start;  // first tile of this block
+  int tiles_x, tiles_y;  // tiles per row and per plane
+};
+
+template <typename S, typename R, int MODEL>
+__global__ void __launch_bounds__(256)
+    k_stream_collide_blocks(const StepParams p, const BlockEntry* __restrict__ blocks,
+                            int nblocks, long long ntiles) {
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    int lo = 0, hi = nblocks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (blocks[mid].tile_start <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const BlockEntry& b = blocks[lo];
+    long long r = t - b.tile_start;
+    const int tx = int(r % b.tiles_x);
+    r /= b.tiles_x;
+    const int ty = int(r % b.tiles_y);
+    const int z = int(r / b.tiles_y);
+    const int x = tx * 32 + threadIdx.x;
+    const int y = ty * blockDim.y + threadIdx.y;
+    if (x < b.g.nx && y < b.g.ny) update_cell<S, R, MODEL>(p, b.g, R(b.omega), x, y, z);
+  }
+}
+
+// Device halo exchange between blocks (BlockLatticeManager::normalCommunicate,
+// block_lattice.hh:1668-1685): after the push, each record copies the listed
+// directions of one neighbour inner cell into one overlap cell.
+struct HaloRec {
+  long long src, dst;  // element offsets within a direction array
+  unsigned int mask;   // bit i: population i crosses the shared face/edge/corner
+};
+
+template <typename S>
+__global__ void k_halo(const HaloRec* __restrict__ recs, int nrecs, S* pops, long long dstride) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrecs; r += gridDim.x * blockDim.x) {
+    const HaloRec h = recs[r];
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+      if (h.mask & (1u << i)) pops[i * dstride + h.dst] = pops[i * dstride + h.src];
   }
 }
 

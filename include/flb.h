@@ -97,6 +97,19 @@ typedef struct flb_lattice_desc {
 
 typedef struct flb_lattice flb_lattice;
 
+/* One block of a multi-block lattice (a BlockLattice of BlockLatticeManager,
+ * src/data_struct/block_lattice.h:234-433; geometry of Block3D,
+ * src/geometry/block_geometry3d.h).  Sizes include the one-cell overlap. */
+typedef struct flb_block_desc {
+  int nx, ny, nz; /* stored cells per axis (interior + 2*overlap) */
+  int ox, oy, oz; /* global stored index of the block's local cell (0,0,0) */
+  double omega;   /* 1/tau of this block; 0 = the lattice descriptor's omega */
+} flb_block_desc;
+
+/* multi-block modes */
+#define FLB_BLOCKS_INDEPENDENT 0 /* separate lattices stepped together (ensemble) */
+#define FLB_BLOCKS_HALO 1        /* blocks of one domain: device halo after each step */
+
 /* Library identification: ABI version and the sm arch the kernels target. */
 FLB_API int flb_version(int* abi_version, int* sm_arch);
 
@@ -113,6 +126,21 @@ FLB_API int flb_desc_default(flb_lattice_desc* d, int nx, int ny, int nz, double
  * initialised to rho0*w_i, RHO to rho0, VELOCITY to 0, flags to 1 (void). */
 FLB_API int flb_create(const flb_lattice_desc* desc, flb_lattice** out);
 FLB_API int flb_destroy(flb_lattice* lat);
+
+/* Allocate `nblocks` blocks in one handle (desc->nx/ny/nz are ignored).
+ * Every block keeps the reference's own streaming (periodic over the block's
+ * linear index).  FLB_BLOCKS_HALO: after each step, overlap cells receive the
+ * populations that cross into the block from the neighbour owning that cell,
+ * as BlockLatticeManager::NormalCommunicate (block_lattice.hh:1419-1430,
+ * 1668-1685; directions of getCommPopDir, communicator.h:76-150), on the
+ * device.  FLB_BLOCKS_INDEPENDENT: blocks are unrelated lattices (the batched
+ * ensemble), each with its own omega.  All blocks advance in one launch per
+ * step through a tile work table. */
+FLB_API int flb_create_blocks(const flb_lattice_desc* desc, int nblocks,
+                              const flb_block_desc* blocks, int mode, flb_lattice** out);
+FLB_API int flb_block_count(const flb_lattice* lat, int* nblocks);
+/* number of halo copy records (overlap cells fed by a neighbour) */
+FLB_API int flb_halo_count(const flb_lattice* lat, long long* nrecords);
 
 /* Device bytes held by the handle. */
 FLB_API int flb_memory_bytes(const flb_lattice* lat, size_t* bytes);
@@ -172,6 +200,38 @@ typedef struct flb_layout {
 } flb_layout;
 FLB_API int flb_get_layout(const flb_lattice* lat, flb_layout* layout);
 FLB_API int flb_device_pointers(flb_lattice* lat, void** pops, void** flags, void** rho, void** vel);
+
+/* Per-block transfers of a multi-block handle (the functions above act on
+ * block 0).  Replace BlockFieldManager::getBlockField(i) and
+ * BlockLatticeManager::getBlockLat(i).getField<...>() access. */
+FLB_API int flb_upload_flags_block(flb_lattice* lat, int block, const uint8_t* host,
+                                   void* stream);
+FLB_API int flb_download_flags_block(flb_lattice* lat, int block, uint8_t* host, void* stream);
+FLB_API int flb_upload_pops_block(flb_lattice* lat, int block, const void* host, int host_dtype,
+                                  void* stream);
+FLB_API int flb_download_pops_block(flb_lattice* lat, int block, void* host, int host_dtype,
+                                    void* stream);
+FLB_API int flb_upload_field_block(flb_lattice* lat, int block, int field, const void* host,
+                                   int host_dtype, void* stream);
+FLB_API int flb_download_field_block(flb_lattice* lat, int block, int field, void* host,
+                                     int host_dtype, void* stream);
+
+/* Launch shape of the stream-collide kernel: tile_y rows of 32 cells per CTA
+ * (1, 2, 4 or 8) and ctas_per_sm resident CTAs per SM for a persistent grid
+ * over the tile work table (0 = one CTA per tile). */
+FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm);
+FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm);
+
+/* Autotuner: times every candidate launch shape for `trial_steps` steps on
+ * `stream` (CUDA events) and keeps the fastest.  The trial steps are real
+ * time steps: the lattice advances by *steps_taken.  best_ms = time per step
+ * of the winner. */
+FLB_API int flb_autotune(flb_lattice* lat, int trial_steps, void* stream, int* tile_y,
+                         int* ctas_per_sm, double* best_ms, int* steps_taken);
+
+/* CUDA-graph stepping: the two-step ping-pong cycle (stream-collide, halo) is
+ * captured once per handle and replayed; equivalent to flb_step. */
+FLB_API int flb_step_graph(flb_lattice* lat, int nsteps, void* stream);
 
 #ifdef __cplusplus
 }

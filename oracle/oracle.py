@@ -224,3 +224,68 @@ def rel_maxnorm(a, b):
     b = np.asarray(b, dtype=np.float64)
     den = np.max(np.abs(b))
     return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0))
+
+
+# --------------------------------------------------------------------------- multi-block
+
+class MultiBlock:
+    """Blocks of one cavity domain, each a restated BlockLattice with its own
+    periodic-shift streaming, followed after every step by the halo copy of
+    BlockLatticeManager::normalCommunicate (src/data_struct/block_lattice.hh:
+    1668-1685): each overlap cell owned by a neighbour's interior receives that
+    neighbour cell's populations in the directions that cross into the block
+    (getCommPopDir, src/parallel/communicator.h:76-150: union over the faces
+    the cell lies beyond)."""
+
+    def __init__(self, blocks, global_flags, n, model="bgk", tau=0.53, ulid=0.1, cs=0.1,
+                 mrt_rate=1.2, dtype=np.float32):
+        self.blocks = blocks
+        self.lats = []
+        gf = np.asarray(global_flags).reshape(n, n, n)
+        for b in blocks:
+            fl = np.ascontiguousarray(gf[b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"],
+                                      b["ox"]:b["ox"] + b["nx"]]).reshape(-1)
+            lat = Lattice(b["nx"], b["ny"], b["nz"], fl, model=model, tau=tau, cs=cs,
+                          mrt_rate=mrt_rate, dtype=dtype)
+            lat.u.reshape(-1, 3)[fl == 8, 0] = lat.dtype.type(ulid)
+            self.lats.append(lat)
+        owner = -np.ones((n, n, n), dtype=np.int64)
+        for k, b in enumerate(blocks):
+            owner[b["oz"] + 1:b["oz"] + b["nz"] - 1, b["oy"] + 1:b["oy"] + b["ny"] - 1,
+                  b["ox"] + 1:b["ox"] + b["nx"] - 1] = k
+        # records grouped per (block, neighbour, direction): (dst idx array, src idx array)
+        self.copies = []
+        for k, b in enumerate(blocks):
+            nx, ny, nz = b["nx"], b["ny"], b["nz"]
+            lz, ly, lx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+            lx, ly, lz = lx.ravel(), ly.ravel(), lz.ravel()
+            outer = (lx == 0) | (ly == 0) | (lz == 0) | (lx == nx - 1) | (ly == ny - 1) | \
+                    (lz == nz - 1)
+            lx, ly, lz = lx[outer], ly[outer], lz[outer]
+            gx, gy, gz = lx + b["ox"], ly + b["oy"], lz + b["oz"]
+            own = owner[gz, gy, gx]
+            keep = own >= 0
+            lx, ly, lz, gx, gy, gz, own = (a[keep] for a in (lx, ly, lz, gx, gy, gz, own))
+            dst = lx + nx * (ly + ny * lz)
+            for i in range(1, 19):
+                cxi, cyi, czi = C[i]
+                cross = np.zeros(lx.size, dtype=bool)
+                for l, m, c in ((lx, nx, cxi), (ly, ny, cyi), (lz, nz, czi)):
+                    cross |= ((l == 0) & (c > 0)) | ((l == m - 1) & (c < 0))
+                for o in np.unique(own[cross]):
+                    sel = cross & (own == o)
+                    nb = blocks[o]
+                    src = (gx[sel] - nb["ox"]) + nb["nx"] * ((gy[sel] - nb["oy"]) +
+                                                            nb["ny"] * (gz[sel] - nb["oz"]))
+                    self.copies.append((k, int(o), i, dst[sel], src))
+
+    def step(self, n=1):
+        for _ in range(n):
+            for lat in self.lats:
+                lat.step(1)
+            for k, o, i, dst, src in self.copies:
+                a, b = self.lats[k], self.lats[o]
+                a.pops[i * a.N + dst] = b.pops[i * b.N + src]
+
+    def rhou_fields(self, key=2):
+        return [lat.rhou_fields(key) for lat in self.lats]

@@ -43,6 +43,25 @@ def small(name, model, ni, tau, ulid, steps, cs, dtype):
     print(name, "written")
 
 
+def multiblock(name, ni, edges, seed, steps, dtype):
+    """Reference multi-block run (BlockReader blocks + NormalCommunicate)."""
+    import tempfile
+    from freelb_b200 import geometry as G
+    blocks = G.uneven_blocks(ni, edges=edges, seed=seed)
+    with tempfile.TemporaryDirectory() as d:
+        bf = os.path.join(d, "blocks.txt")
+        G.write_block_file(bf, blocks)
+        r = O.run_reference("bgk", ni, 0.53, 0.1, steps, 0, dtype=dtype, blockfile=bf,
+                            threads=4)
+    out = {"params": np.array([ni, 0.53, 0.1, steps, seed], dtype=np.float64),
+           "edges": np.array(edges), "nblocks": np.array(len(blocks))}
+    for k in range(len(blocks)):
+        for f in ("flags", "pops", "rho", "u"):
+            out[f"{f}_b{k}"] = r[f"{f}_b{k}"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "written,", len(blocks), "blocks")
+
+
 def c1():
     ni, steps = 100, 1000
     r = O.run_reference("bgk", ni, 0.53, 0.1, steps, 0, dtype=np.float32)
@@ -62,5 +81,7 @@ def c1():
 if __name__ == "__main__":
     for case in SMALL:
         small(*case)
+    multiblock("blocks_bgk_f64_n12_s30", 12, (4, 8), 3, 30, np.float64)
+    multiblock("blocks_bgk_f32_n12_s30", 12, (4, 8), 3, 30, np.float32)
     if "--no-c1" not in sys.argv:
         c1()

@@ -1,0 +1,136 @@
+"""GPU tests of multi-block lattices: device halo exchange (uneven blocks of
+one cavity), the batched ensemble of independent cavities, launch-shape
+control, the autotuner and CUDA-graph stepping."""
+import numpy as np
+import pytest
+
+import freelb_b200 as F
+from conftest import golden, rel_maxnorm
+from freelb_b200 import geometry as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_blocks(ni, blocks, storage="fp32", tau=0.53, ulid=0.1):
+    n = ni + 2
+    flags = F.cavity_flags(ni)
+    lat = F.Lattice.blocks(G.block_tuples(blocks), tau, mode="halo", storage=storage)
+    real = lat.real
+    u = np.zeros((n ** 3, 3), dtype=real)
+    u[flags == 8, 0] = real(ulid)
+    for k, b in enumerate(blocks):
+        lat.upload_flags(G.slice_block(flags, n, b), block=k)
+        lat.upload_field("u", G.slice_block(u, n, b, comps=3), block=k)
+    return lat
+
+
+@pytest.mark.parametrize("name", ["blocks_bgk_f64_n12_s30", "blocks_bgk_f32_n12_s30"])
+def test_blocks_match_reference_multiblock_golden(gpu_ok, name):
+    g = golden(name)
+    ni, _, _, steps, seed = g["params"]
+    blocks = G.uneven_blocks(int(ni), edges=tuple(int(e) for e in g["edges"]), seed=int(seed))
+    storage = "fp64" if "f64" in name else "fp32"
+    lat = gpu_blocks(int(ni), blocks, storage)
+    assert lat.halo_count() > 0
+    lat.step(int(steps))
+    lat.compute_rhou(2)
+    tol = 1e-12 if storage == "fp64" else 1e-5
+    pops = np.concatenate([lat.download_pops(block=k) for k in range(len(blocks))])
+    ref = np.concatenate([g[f"pops_b{k}"] for k in range(len(blocks))])
+    assert rel_maxnorm(pops, ref) < tol
+    u = np.concatenate([lat.download_field("u", block=k) for k in range(len(blocks))])
+    uref = np.concatenate([g[f"u_b{k}"] for k in range(len(blocks))])
+    assert rel_maxnorm(u, uref) < tol
+    for k in range(len(blocks)):
+        assert np.array_equal(lat.download_flags(block=k), g[f"flags_b{k}"])
+
+
+@pytest.mark.parametrize("tile_y,ctas", [(8, 0), (2, 4), (1, 0)])
+def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas):
+    """Uneven blocks with device halos reproduce the single-block run exactly on
+    fluid cells, for every launch shape."""
+    ni = 40
+    blocks = G.uneven_blocks(ni, edges=(8, 12, 16), seed=5)
+    lat = gpu_blocks(ni, blocks, "fp32")
+    lat.set_launch(tile_y, ctas)
+    lat.step(40)
+    one = F.cavity(ni)
+    one.step(40)
+    n = ni + 2
+    P = one.download_pops().reshape(19, n, n, n)
+    for k, b in enumerate(blocks):
+        pb = lat.download_pops(block=k).reshape(19, b["nz"], b["ny"], b["nx"])
+        fb = G.slice_block(F.cavity_flags(ni), n, b).reshape(b["nz"], b["ny"], b["nx"])
+        ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
+        assert np.array_equal(pb[:, fb == 2], ps[:, fb == 2])
+
+
+def test_blocks_vs_oracle_multiblock_fp64(gpu_ok):
+    ni = 18
+    blocks = G.uneven_blocks(ni, edges=(4, 6, 8), seed=9)
+    lat = gpu_blocks(ni, blocks, "fp64", tau=0.56, ulid=0.08)
+    mb = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, tau=0.56, ulid=0.08, dtype=np.float64)
+    lat.step(33)
+    mb.step(33)
+    ours = np.concatenate([lat.download_pops(block=k) for k in range(len(blocks))])
+    ref = np.concatenate([m.pops for m in mb.lats])
+    assert rel_maxnorm(ours, ref) < 1e-12
+
+
+def ensemble(sizes, taus, storage="fp32", ulid=0.1):
+    lat = F.Lattice.blocks([(n + 2, n + 2, n + 2, 0, 0, 0, 1.0 / t) for n, t in zip(sizes, taus)],
+                           0.6, mode="independent", storage=storage)
+    for k, n in enumerate(sizes):
+        fl = F.cavity_flags(n)
+        u = np.zeros(((n + 2) ** 3, 3), dtype=lat.real)
+        u[fl == 8, 0] = lat.real(ulid)
+        lat.upload_flags(fl, block=k)
+        lat.upload_field("u", u, block=k)
+    return lat
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_ensemble_each_cavity_matches_single(gpu_ok, graph):
+    """Batched independent cavities, each with its own tau, match one-at-a-time runs."""
+    rng = np.random.default_rng(1)
+    sizes = [int(v) for v in rng.integers(6, 20, size=9)]
+    taus = [0.5 + 3 * 0.1 * n / float(np.exp(rng.uniform(np.log(100), np.log(3000))))
+            for n in sizes]
+    lat = ensemble(sizes, taus)
+    lat.step(25, graph=graph)
+    for k, (n, t) in enumerate(zip(sizes, taus)):
+        ref = O.cavity(n, tau=t, ulid=0.1)
+        ref.step(25)
+        assert rel_maxnorm(lat.download_pops(block=k), ref.pops) < 1e-5, (k, n, t)
+
+
+def test_graph_step_equals_plain_step(gpu_ok):
+    a = F.cavity(30)
+    b = F.cavity(30)
+    a.step(17)
+    b.step(17, graph=True)
+    assert np.array_equal(a.download_pops(), b.download_pops())
+    a.step(4, graph=True)
+    b.step(4)
+    assert np.array_equal(a.download_pops(), b.download_pops())
+
+
+def test_autotune_keeps_results_exact(gpu_ok):
+    a = F.cavity(36)
+    b = F.cavity(36)
+    ty, c, ms, taken = a.autotune(trial_steps=2)
+    assert ty in (1, 2, 4, 8) and c in (0, 2, 4, 8) and ms > 0 and taken > 0
+    assert a.get_launch() == (ty, c)
+    b.step(taken)
+    a.step(5)
+    b.step(5)
+    assert np.array_equal(a.download_pops(), b.download_pops())
+
+
+def test_set_launch_rejects_bad_shapes(gpu_ok):
+    a = F.cavity(8)
+    with pytest.raises(F.FlbError):
+        a.set_launch(3, 0)
+    with pytest.raises(F.FlbError):
+        a.set_launch(8, -1)

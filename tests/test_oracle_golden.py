@@ -95,3 +95,54 @@ def test_restatement_matches_live_reference(model):
     assert np.array_equal(lat.flags, r["flags"])
     assert rel_maxnorm(lat.pops, r["pops"]) < 1e-12
     assert rel_maxnorm(u, r["u"]) < 1e-12
+
+
+def _blocks_from_golden(g):
+    from freelb_b200 import geometry as G
+    ni, _, _, _, seed = g["params"]
+    return G.uneven_blocks(int(ni), edges=tuple(int(e) for e in g["edges"]), seed=int(seed))
+
+
+@pytest.mark.parametrize("name", ["blocks_bgk_f64_n12_s30", "blocks_bgk_f32_n12_s30"])
+def test_multiblock_restatement_matches_reference(name):
+    """BlockReader blocks + NormalCommunicate, restated, against the reference run."""
+    g = golden(name)
+    blocks = _blocks_from_golden(g)
+    assert len(blocks) == int(g["nblocks"])
+    dtype = np.float64 if "f64" in name else np.float32
+    ni = int(g["params"][0])
+    mb = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, dtype=dtype)
+    mb.step(int(g["params"][3]))
+    fields = mb.rhou_fields()
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    ours = np.concatenate([mb.lats[k].pops for k in range(len(blocks))])
+    ref = np.concatenate([g[f"pops_b{k}"] for k in range(len(blocks))])
+    assert rel_maxnorm(ours, ref) < tol
+    u = np.concatenate([fields[k][1] for k in range(len(blocks))])
+    uref = np.concatenate([g[f"u_b{k}"] for k in range(len(blocks))])
+    assert rel_maxnorm(u, uref) < tol
+    for k in range(len(blocks)):
+        assert np.array_equal(mb.lats[k].flags, g[f"flags_b{k}"])
+
+
+def test_multiblock_equals_single_block_on_fluid_cells():
+    from freelb_b200 import geometry as G
+    blocks = G.uneven_blocks(16, edges=(4, 6, 8), seed=11)
+    mb = O.MultiBlock(blocks, O.cavity_flags(16), 18, dtype=np.float64)
+    mb.step(25)
+    sb = O.cavity(16, dtype=np.float64)
+    sb.step(25)
+    P = sb.pops.reshape(19, 18, 18, 18)
+    for k, b in enumerate(blocks):
+        pb = mb.lats[k].pops.reshape(19, b["nz"], b["ny"], b["nx"])
+        fb = mb.lats[k].flags.reshape(b["nz"], b["ny"], b["nx"])
+        ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
+        assert np.array_equal(pb[:, fb == 2], ps[:, fb == 2])
+
+
+def test_partition_axis_tiles_exactly():
+    import random
+    from freelb_b200 import geometry as G
+    for seed in range(20):
+        p = G.partition_axis(256, (32, 48, 64, 96), random.Random(seed))
+        assert sum(p) == 256 and set(p) <= {32, 48, 64, 96}
