@@ -163,6 +163,179 @@ def run_reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- our arm
 
+class DeviceTimer:
+    """CUDA events on the launching stream, synchronised on both sides."""
+
+    def __init__(self, torch, stream):
+        self.torch, self.stream = torch, stream
+
+    def __enter__(self):
+        self.torch.cuda.synchronize()
+        self.e0 = self.torch.cuda.Event(enable_timing=True)
+        self.e1 = self.torch.cuda.Event(enable_timing=True)
+        self.e0.record(self.stream)
+        return self
+
+    def __exit__(self, *exc):
+        self.e1.record(self.stream)
+        self.torch.cuda.synchronize()
+        self.ms = self.e0.elapsed_time(self.e1)
+
+
+def timed_cavity(F, torch, stream, ni, steps, warmup, storage="fp32", model="bgk", tune=True,
+                 tau=0.53, smagorinsky=0.1):
+    """Cavity of ni^3 interior cells: autotune the launch shape (the tuning steps
+    are real warm-up steps), then time `steps` steps.  Returns (ms, launch, lat)."""
+    lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model, smagorinsky=smagorinsky)
+    launch = None
+    if tune:
+        launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
+    for _ in range(warmup):
+        lat.step(1, stream)
+    with DeviceTimer(torch, stream) as t:
+        lat.step(steps, stream)
+    return t.ms, launch, lat
+
+
+def accuracy_block(F, ni, steps):
+    """Relative L2 error of u after `steps` steps against an FP64 run of the same
+    kernel, per model and storage (C2 accuracy report)."""
+    out = {}
+    for model, tau in (("bgk", 0.53), ("mrt", 0.53), ("les", 3 * 0.1 * ni / 10000 + 0.5)):
+        us = {}
+        for storage in ("fp64", "fp32", "fp16s"):
+            lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model)
+            lat.step(steps)
+            _, u = lat.rhou(key=2, dtype=np.float64)
+            us[storage] = u
+            lat.close()
+        ref = np.linalg.norm(us["fp64"])
+        out[model] = {"tau": tau,
+                      "fp32_rel_l2_u": float(np.linalg.norm(us["fp32"] - us["fp64"]) / ref),
+                      "fp16s_rel_l2_u": float(np.linalg.norm(us["fp16s"] - us["fp64"]) / ref)}
+    return {"config": f"{ni}^3 cavity, {steps} steps, u_lid=0.1 (LES: Cs=0.1, Re=10000)",
+            "models": out}
+
+
+def blocks_block(F, torch, stream, ni, steps, seed=0):
+    """Uneven-block 256^3 cavity with device halos vs the single-block run."""
+    from freelb_b200 import geometry as G
+    blocks = G.uneven_blocks(ni, edges=(32, 48, 64, 96), seed=seed)
+    n = ni + 2
+    flags = F.cavity_flags(ni)
+    lat = F.Lattice.blocks(G.block_tuples(blocks), 0.53, mode="halo")
+    u = np.zeros((n ** 3, 3), dtype=np.float32)
+    u[flags == 8, 0] = np.float32(0.1)
+    for k, b in enumerate(blocks):
+        lat.upload_flags(G.slice_block(flags, n, b), block=k)
+        lat.upload_field("u", G.slice_block(u, n, b, comps=3), block=k)
+    launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
+    with DeviceTimer(torch, stream) as t:
+        lat.step(steps, stream)
+    stored = sum(b["nx"] * b["ny"] * b["nz"] for b in blocks)
+    res = {"blocks": len(blocks), "stored_cells": stored, "halo_records": lat.halo_count(),
+           "launch": launch, "glups_stored": stored * steps / (t.ms / 1e3) / 1e9,
+           "glups_domain": n ** 3 * steps / (t.ms / 1e3) / 1e9}
+    lat.close()
+    return res
+
+
+def ensemble_block(F, torch, stream, steps, count=128, seed=0):
+    """128 independent cavities (n ~ U{32..128}, Re ~ logU[100, 3000],
+    tau = 3 u_lid n / Re + 0.5) in one multi-block handle (tile work table,
+    autotuned, CUDA-graph stepping) against one handle per cavity stepped one
+    after another."""
+    rng = np.random.default_rng(seed)
+    sizes = [int(v) for v in rng.integers(32, 129, size=count)]
+    res_ = np.exp(rng.uniform(np.log(100.0), np.log(3000.0), size=count))
+    taus = [3 * 0.1 * n / r + 0.5 for n, r in zip(sizes, res_)]
+    cells = sum((n + 2) ** 3 for n in sizes)
+    out = {"cavities": count, "stored_cells": cells, "steps": steps}
+    for storage in ("fp32", "fp16s"):
+        lat = F.Lattice.blocks([(n + 2, n + 2, n + 2, 0, 0, 0, 1.0 / t)
+                                for n, t in zip(sizes, taus)], 0.6, mode="independent",
+                               storage=storage)
+        for k, n in enumerate(sizes):
+            fl = F.cavity_flags(n)
+            u = np.zeros(((n + 2) ** 3, 3), dtype=lat.real)
+            u[fl == 8, 0] = lat.real(0.1)
+            lat.upload_flags(fl, block=k)
+            lat.upload_field("u", u, block=k)
+        launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
+        lat.step(2, stream, graph=True)
+        with DeviceTimer(torch, stream) as t:
+            lat.step(steps, stream, graph=True)
+        out[storage] = {"batched_glups": cells * steps / (t.ms / 1e3) / 1e9, "launch": launch}
+        lat.close()
+    # one-at-a-time: a handle per cavity, each stepped `steps` times in turn
+    lats = [F.cavity(n, tau=t, ulid=0.1) for n, t in zip(sizes, taus)]
+    for lat in lats:
+        lat.step(1, stream)
+    with DeviceTimer(torch, stream) as t:
+        for _ in range(steps):
+            for lat in lats:
+                lat.step(1, stream)
+    out["fp32"]["sequential_glups"] = cells * steps / (t.ms / 1e3) / 1e9
+    for lat in lats:
+        lat.close()
+    return out
+
+
+def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=2, seed=0):
+    """C5: 128^3 cavity, Re = 500 (tau = 3*0.1*128/500 + 0.5), porosity alpha ~
+    U[0, 0.05]; J = sum |u|^2 at T = 2000; checkpoints every 100 steps; FP32
+    forward and adjoint, FP64 gradient accumulation.  Reports the adjoint-to-
+    forward time ratio and the gradient's relative error against FP64 central
+    differences (h = 1e-4) on a few seeded cells and on tau."""
+    tau = 3 * 0.1 * ni / 500 + 0.5
+    n = ni + 2
+    alpha = np.random.default_rng(seed).uniform(0.0, 0.05, size=n ** 3)
+
+    def lattice(storage, a=alpha, t=tau):
+        lat = F.cavity(ni, tau=t, ulid=0.1, storage=storage, model="brinkman")
+        lat.upload_field("alpha", a.astype(lat.real))
+        return lat
+
+    lat = lattice("fp32")
+    with DeviceTimer(torch, stream) as tf:
+        lat.step(steps, stream)
+    lat.close()
+    lat = lattice("fp32")
+    with DeviceTimer(torch, stream) as tfc:
+        lat.adjoint_forward(steps, every, stream)
+    with DeviceTimer(torch, stream) as tb:
+        g_alpha, g_tau, g_ulid = lat.adjoint_backward(stream=stream)
+    lat.close()
+
+    def J(a=alpha, t=tau):
+        m = lattice("fp64", a, t)
+        m.step(steps, stream)
+        v = m.objective_u2(stream)
+        m.close()
+        return v
+
+    h = 1e-4
+    flags = F.cavity_flags(ni)
+    fluid = np.flatnonzero(flags == 2)
+    cells = np.random.default_rng(seed + 1).choice(fluid, size=fd_cells, replace=False)
+    errs = []
+    for c in cells:
+        ap, am = alpha.copy(), alpha.copy()
+        ap[c] += h
+        am[c] -= h
+        fd = (J(ap) - J(am)) / (2 * h)
+        errs.append(abs(g_alpha[c] - fd) / abs(fd))
+    fd_tau = (J(t=tau + h) - J(t=tau - h)) / (2 * h)
+    return {"config": f"{ni}^3, T={steps}, checkpoints every {every}, tau={tau:.4f}",
+            "forward_ms_per_step": tf.ms / steps,
+            "forward_with_checkpoints_ms_per_step": tfc.ms / steps,
+            "backward_ms_per_step": tb.ms / steps,
+            "adjoint_to_forward_ratio": tb.ms / tf.ms,
+            "dJ_dtau": g_tau, "dJ_dulid": g_ulid,
+            "fd_rel_err_alpha": [float(e) for e in errs],
+            "fd_rel_err_tau": float(abs(g_tau - fd_tau) / abs(fd_tau))}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import freelb_b200 as F
@@ -180,32 +353,33 @@ def run_ours(args, rank, world, local_rank):
     cells = n ** 3
     stream = torch.cuda.current_stream(dev)
 
-    def timed(storage, model="bgk"):
-        lat = F.cavity(ni, tau=0.53, ulid=0.1, storage=storage, model=model)
-        for _ in range(args.warmup):
-            lat.step(1, stream)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        with ClockSampler(local_rank) as cs:
-            e0.record(stream)
-            lat.step(args.steps, stream)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        finite = lat.nonfinite()
-        lat.close()
-        return ms, cs.summary(), finite
+    def max_over_ranks(ms):
+        if not dist:
+            return ms
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
-    ms32, clocks, bad32 = timed("fp32")
-    ms16, clocks16, bad16 = timed("fp16s")
+    # headline: 512^3 BGK FP32, launch shape from the autotuner
+    lat = F.cavity(ni, tau=0.53, ulid=0.1, storage=args.storage)
+    if args.launch:
+        launch = tuple(int(v) for v in args.launch.split(","))
+        lat.set_launch(*launch)
+    else:
+        launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
+    for _ in range(args.warmup):
+        lat.step(1, stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as cs:
+        with DeviceTimer(torch, stream) as t:
+            lat.step(args.steps, stream)
+    ms32 = max_over_ranks(t.ms)
+    clocks = cs.summary()
+    bad32 = lat.nonfinite()
+    lat.close()
 
     # end to end through the public API with host buffers: flags + lid velocity
     # field in from pinned host memory, K steps, RHO and VELOCITY back out.
@@ -216,38 +390,56 @@ def run_ours(args, rank, world, local_rank):
     pin_u = torch.from_numpy(u0.reshape(-1)).pin_memory().numpy()
     out_rho = torch.empty(cells, dtype=torch.float32).pin_memory().numpy()
     out_u = torch.empty(3 * cells, dtype=torch.float32).pin_memory().numpy()
-    lat = F.Lattice(n, n, n, 0.53, storage="fp32")
+    if args.storage == "fp64":
+        pin_u = torch.from_numpy(u0.reshape(-1).astype(np.float64)).pin_memory().numpy()
+    lat = F.Lattice(n, n, n, 0.53, storage=args.storage)
+    lat.set_launch(*launch)
     lat.step(1, stream)  # first-launch costs outside the timed region
     lat.init_equilibrium(1.0, stream)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    lat.upload_flags(pin_flags, stream)
-    lat.upload_field("u", pin_u, stream)
-    lat.step(args.steps, stream)
-    lat.compute_rhou(2, stream)
-    import ctypes
-    from freelb_b200 import _capi as C
-    C.call("flb_download_field", lat._h, C.FIELD_RHO, ctypes.c_void_p(out_rho.ctypes.data),
-           C.DTYPE_F32, ctypes.c_void_p(stream.cuda_stream))
-    C.call("flb_download_field", lat._h, C.FIELD_VELOCITY, ctypes.c_void_p(out_u.ctypes.data),
-           C.DTYPE_F32, ctypes.c_void_p(stream.cuda_stream))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    wall_ms = (time.perf_counter() - t0) * 1000.0
-    e2e_ms = max(e2e_ms, wall_ms)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    with DeviceTimer(torch, stream) as te:
+        lat.upload_flags(pin_flags, stream)
+        lat.upload_field("u", pin_u, stream)
+        lat.step(args.steps, stream)
+        lat.compute_rhou(2, stream)
+        import ctypes
+        from freelb_b200 import _capi as C
+        C.call("flb_download_field", lat._h, C.FIELD_RHO, ctypes.c_void_p(out_rho.ctypes.data),
+               C.DTYPE_F32, ctypes.c_void_p(stream.cuda_stream))
+        C.call("flb_download_field", lat._h, C.FIELD_VELOCITY,
+               ctypes.c_void_p(out_u.ctypes.data), C.DTYPE_F32,
+               ctypes.c_void_p(stream.cuda_stream))
+    e2e_ms = max_over_ranks(max(te.ms, (time.perf_counter() - t0) * 1000.0))
     lat.close()
     h2d = flags.nbytes + u0.nbytes
     d2h = out_rho.nbytes + out_u.nbytes
+
+    extras = {}
+    if world == 1 and not args.quick:
+        # other models and storages on the same 512^3 cavity
+        variants = {}
+        les_tau = 3 * 0.1 * ni / 10000 + 0.5
+        for storage, model, tau in (("fp16s", "bgk", 0.53), ("fp32", "mrt", 0.53),
+                                    ("fp16s", "mrt", 0.53), ("fp32", "les", les_tau),
+                                    ("fp16s", "les", les_tau), ("fp64", "bgk", 0.53)):
+            ms, lch, vl = timed_cavity(F, torch, stream, ni, args.steps, 2, storage, model,
+                                       tau=tau)
+            bad = vl.nonfinite()
+            vl.close()
+            b = algo_bytes_per_cell(storage)
+            ach = cells * b / (ms / args.steps / 1e3) / 1e9
+            variants[f"{model}_{storage}"] = {
+                "glups": cells * args.steps / (ms / 1e3) / 1e9, "ms_per_step": ms / args.steps,
+                "launch": lch, "achieved_gbs": ach, "frac": ach / measured_peaks()[0],
+                "algorithmic_bytes_per_cell": b, "tau": tau, "nonfinite": bad}
+        extras["variants"] = variants
+        extras["accuracy"] = accuracy_block(F, 256, 2000)
+        extras["blocks_256"] = blocks_block(F, torch, stream, 256, args.steps)
+        extras["ensemble_128"] = ensemble_block(F, torch, stream, args.steps)
+        extras["adjoint_128"] = adjoint_block(F, torch, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -261,15 +453,10 @@ def run_ours(args, rank, world, local_rank):
 
     peak, peak_kind = measured_peaks()
     glups32 = cells * args.steps * world / (ms32 / 1000.0) / 1e9
-    glups16 = cells * args.steps * world / (ms16 / 1000.0) / 1e9
-    b32 = algo_bytes_per_cell("fp32")
-    b16 = algo_bytes_per_cell("fp16s")
+    b32 = algo_bytes_per_cell(args.storage)
     per_launch_ms32 = ms32 / args.steps
-    per_launch_ms16 = ms16 / args.steps
     ach32 = cells * b32 / (per_launch_ms32 / 1000.0) / 1e9
-    ach16 = cells * b16 / (per_launch_ms16 / 1000.0) / 1e9
-    tr32 = profile_traffic("fp32_bgk_bytes_per_cell")
-    tr16 = profile_traffic("fp16s_bgk_bytes_per_cell")
+    tr32 = profile_traffic(f"{args.storage}_bgk_bytes_per_cell")
     line = {
         "metric": "D3Q19 cavity GLUPs (stored cells)",
         "value": glups32,
@@ -281,22 +468,16 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": {"fp32": "f32", "fp16s": "f32 (fp16 storage)", "fp64": "f64"}[args.storage],
         "data": "synthetic",
         "config": {"workload": f"lid-driven cavity {ni}^3 D3Q19 BGK tau=0.53 u_lid=0.1",
-                   "stored_cells": cells, "storage": "fp32", "per_gpu": "independent cavity",
+                   "stored_cells": cells, "storage": args.storage, "per_gpu": "independent cavity",
                    "l2": "working set 21.8 GB >> 126 MB L2; no flush needed",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}", "launch": launch},
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
                      "frac": ach32 / peak, "peak_source": peak_kind,
                      "traffic": (tr32 * cells if tr32 else None),
                      "algorithmic_bytes_per_cell": b32},
-        "fp16s": {"value": glups16, "unit": "GLUPs", "ms_per_step": ms16 / args.steps,
-                  "roofline": {"achieved": ach16, "peak": peak, "unit": "GB/s",
-                               "frac": ach16 / peak,
-                               "traffic": (tr16 * cells if tr16 else None),
-                               "algorithmic_bytes_per_cell": b16},
-                  "clocks": clocks16, "nonfinite": bad16},
         "e2e": {"value": cells * args.steps * world / (e2e_ms / 1000.0) / 1e9, "unit": "GLUPs",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "job": "flags + VELOCITY in (pinned host), K steps, RHO + VELOCITY out"},
@@ -304,6 +485,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "nonfinite": bad32,
     }
+    line.update(extras)
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["mlups"] / 1000.0, "unit": "GLUPs",
                                 "cores": cpu["threads"], "kind": "reference",
@@ -320,6 +502,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ni", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "fp64"],
+                    help="population storage of the headline run (profiling)")
+    ap.add_argument("--launch", default=None,
+                    help="tile_y,ctas_per_sm,cells_per_thread for the headline run instead of "
+                         "the autotuner (profiling)")
+    ap.add_argument("--quick", action="store_true",
+                    help="headline and e2e only (no variants / accuracy / blocks / ensemble / "
+                         "adjoint blocks)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

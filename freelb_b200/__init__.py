@@ -16,7 +16,9 @@ from . import _capi as C
 from ._capi import FlbError  # noqa: F401
 
 STORAGES = {"fp32": C.STORAGE_FP32, "fp16s": C.STORAGE_FP16S, "fp64": C.STORAGE_FP64}
-MODELS = {"bgk": C.MODEL_BGK, "mrt": C.MODEL_MRT, "les": C.MODEL_LES}
+MODELS = {"bgk": C.MODEL_BGK, "mrt": C.MODEL_MRT, "les": C.MODEL_LES,
+          "brinkman": C.MODEL_BRINKMAN}
+FIELDS = {"rho": C.FIELD_RHO, "u": C.FIELD_VELOCITY, "alpha": C.FIELD_ALPHA}
 OPS = {"none": C.OP_NONE, "bulk": C.OP_BULK, "bounceback": C.OP_BOUNCEBACK,
        "movingwall": C.OP_MOVINGWALL, "field_bgk": C.OP_FIELD_BGK}
 
@@ -156,19 +158,19 @@ class Lattice:
         return p
 
     def upload_field(self, name, values, stream=None, block=0):
-        fid = C.FIELD_RHO if name == "rho" else C.FIELD_VELOCITY
+        fid = FIELDS[name]
         n = self.ncells(block)
         v = np.ascontiguousarray(values).reshape(-1)
-        assert v.size == (n if fid == C.FIELD_RHO else 3 * n)
+        assert v.size == (3 * n if fid == C.FIELD_VELOCITY else n)
         dt = C.DTYPE_F64 if v.dtype == np.float64 else C.DTYPE_F32
         v = v.astype(np.float64 if dt == C.DTYPE_F64 else np.float32, copy=False)
         C.call("flb_upload_field_block", self._h, block, fid, _ptr(v), dt, _stream(stream))
 
     def download_field(self, name, dtype=None, stream=None, block=0):
-        fid = C.FIELD_RHO if name == "rho" else C.FIELD_VELOCITY
+        fid = FIELDS[name]
         dtype = np.dtype(dtype or self.real)
         n = self.ncells(block)
-        v = np.empty(n if fid == C.FIELD_RHO else 3 * n, dtype=dtype)
+        v = np.empty(3 * n if fid == C.FIELD_VELOCITY else n, dtype=dtype)
         dt = C.DTYPE_F64 if dtype == np.float64 else C.DTYPE_F32
         C.call("flb_download_field_block", self._h, block, fid, _ptr(v), dt, _stream(stream))
         return v
@@ -180,21 +182,23 @@ class Lattice:
     def step(self, n=1, stream=None, graph=False):
         C.call("flb_step_graph" if graph else "flb_step", self._h, int(n), _stream(stream))
 
-    def set_launch(self, tile_y=8, ctas_per_sm=0):
-        C.call("flb_set_launch", self._h, int(tile_y), int(ctas_per_sm))
+    def set_launch(self, tile_y=8, ctas_per_sm=0, cells_per_thread=0):
+        C.call("flb_set_launch", self._h, int(tile_y), int(ctas_per_sm), int(cells_per_thread))
 
     def get_launch(self):
-        a, b = ctypes.c_int(), ctypes.c_int()
-        C.call("flb_get_launch", self._h, ctypes.byref(a), ctypes.byref(b))
-        return a.value, b.value
+        """(tile_y, ctas_per_sm, cells_per_thread)."""
+        a, b, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        C.call("flb_get_launch", self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(v))
+        return a.value, b.value, v.value
 
     def autotune(self, trial_steps=4, stream=None):
-        """Pick the fastest launch shape; returns (tile_y, ctas_per_sm, ms/step, steps run)."""
-        ty, c, steps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        """Pick the fastest launch shape; returns
+        ((tile_y, ctas_per_sm, cells_per_thread), ms per step, steps run)."""
+        ty, c, v, steps = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         ms = ctypes.c_double()
         C.call("flb_autotune", self._h, int(trial_steps), _stream(stream), ctypes.byref(ty),
-               ctypes.byref(c), ctypes.byref(ms), ctypes.byref(steps))
-        return ty.value, c.value, ms.value, steps.value
+               ctypes.byref(c), ctypes.byref(v), ctypes.byref(ms), ctypes.byref(steps))
+        return (ty.value, c.value, v.value), ms.value, steps.value
 
     def compute_rhou(self, key=2, stream=None):
         C.call("flb_compute_rhou", self._h, int(key), _stream(stream))
@@ -218,6 +222,32 @@ class Lattice:
         v = ctypes.c_uint64()
         C.call("flb_check_finite", self._h, ctypes.byref(v), _stream(stream))
         return int(v.value)
+
+    # -- objective and discrete adjoint
+    def objective_u2(self, stream=None):
+        """J = sum over bulk cells of |u|^2 (forced moment with the alpha field)."""
+        v = ctypes.c_double()
+        C.call("flb_objective_u2", self._h, ctypes.byref(v), _stream(stream))
+        return v.value
+
+    def adjoint_forward(self, nsteps, checkpoint_every=100, stream=None):
+        """Advance nsteps keeping checkpoints; returns J at the end."""
+        v = ctypes.c_double()
+        C.call("flb_adjoint_forward", self._h, int(nsteps), int(checkpoint_every),
+               ctypes.byref(v), _stream(stream))
+        return v.value
+
+    def adjoint_backward(self, alpha_grad=True, stream=None):
+        """Gradients of the last adjoint_forward objective:
+        (dJ/dalpha per cell or None, dJ/dtau, dJ/du_lid)."""
+        g = np.empty(self.N, dtype=np.float64) if alpha_grad else None
+        t, u = ctypes.c_double(), ctypes.c_double()
+        C.call("flb_adjoint_backward", self._h, _ptr(g) if g is not None else None,
+               ctypes.byref(t), ctypes.byref(u), _stream(stream))
+        return g, t.value, u.value
+
+    def adjoint_release(self):
+        C.call("flb_adjoint_release", self._h)
 
     def layout(self):
         L = C.Layout()

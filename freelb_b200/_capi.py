@@ -16,10 +16,10 @@ ERRORS = {-1: "FLB_ERR_INVALID", -2: "FLB_ERR_CUDA", -3: "FLB_ERR_OOM", -4: "FLB
           -5: "FLB_ERR_NUMERIC", -6: "FLB_ERR_UNSUPPORTED", -7: "FLB_ERR_STATE"}
 
 STORAGE_FP32, STORAGE_FP16S, STORAGE_FP64 = 0, 1, 2
-MODEL_BGK, MODEL_MRT, MODEL_LES = 0, 1, 2
+MODEL_BGK, MODEL_MRT, MODEL_LES, MODEL_BRINKMAN = 0, 1, 2, 3
 OP_NONE, OP_BULK, OP_BOUNCEBACK, OP_MOVINGWALL, OP_FIELD_BGK = 0, 1, 2, 3, 4
 DTYPE_F32, DTYPE_F64 = 0, 1
-FIELD_RHO, FIELD_VELOCITY = 0, 1
+FIELD_RHO, FIELD_VELOCITY, FIELD_ALPHA = 0, 1, 2
 MAX_TASKS = 8
 
 
@@ -88,11 +88,17 @@ SIGNATURES = {
     "flb_download_pops_block": [_P, _I, _P, _I, _P],
     "flb_upload_field_block": [_P, _I, _I, _P, _I, _P],
     "flb_download_field_block": [_P, _I, _I, _P, _I, _P],
-    "flb_set_launch": [_P, _I, _I],
-    "flb_get_launch": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)],
-    "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I),
+    "flb_set_launch": [_P, _I, _I, _I],
+    "flb_get_launch": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)],
     "flb_step_graph": [_P, _I, _P],
+    "flb_objective_u2": [_P, ctypes.POINTER(ctypes.c_double), _P],
+    "flb_adjoint_forward": [_P, _I, _I, ctypes.POINTER(ctypes.c_double), _P],
+    "flb_adjoint_backward": [_P, _P, ctypes.POINTER(ctypes.c_double),
+                             ctypes.POINTER(ctypes.c_double), _P],
+    "flb_adjoint_release": [_P],
+    "flb_set_tasks": [_P, _I, _P, _P, _I],
 }
 _RESTYPES = {"flb_last_error": ctypes.c_char_p}
 

@@ -61,5 +61,27 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+EXAMPLE_SRC = os.path.join(HERE, "cpp", "examples", "cavity3d_b200.cpp")
+EXAMPLE_BIN = os.path.join(HERE, "cpp", "_build", "cavity3d_b200")
+
+
+def build_examples(force: bool = False) -> str:
+    """Compile the C++17 host-class example against libflb_b200.so (g++)."""
+    deps = [EXAMPLE_SRC, os.path.join(HERE, "cpp", "freelb.h"), LIB]
+    if not force and not _stale(EXAMPLE_BIN, deps):
+        return EXAMPLE_BIN
+    os.makedirs(os.path.dirname(EXAMPLE_BIN), exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-o", EXAMPLE_BIN, EXAMPLE_SRC, "-L" + HERE, "-lflb_b200",
+           "-Wl,-rpath,$ORIGIN/../.."]
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    res = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    return EXAMPLE_BIN
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_examples(force="--force" in sys.argv))

@@ -21,7 +21,7 @@
 #include <vector>
 
 #include "../../include/flb.h"
-#include "flb_kernels.cuh"
+#include "flb_adjoint.cuh"
 
 using namespace flb;
 
@@ -89,12 +89,22 @@ struct flb_lattice {
   BlockEntry* d_blocks = nullptr;
   long long ntiles = 0;
   int table_tile_y = 0;
-  HaloRec* d_halo = nullptr;
+  int table_vec = 0;
+  HaloCopy* d_halo = nullptr;
   long long nhalo = 0;
-  int tile_y = 8;
+  int tile_y = 4;
   int ctas_per_sm = 0;
+  int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // Brinkman porosity (FLB_FIELD_ALPHA), arithmetic type
+  void* alpha = nullptr;
+  // adjoint workspace
+  int adj_T = 0, adj_k = 0;
+  std::vector<void*> adj_ckpt;  // Q_0, Q_k, Q_2k, ...
+  std::vector<void*> adj_seg;   // recomputed Q_{t0+1} .. Q_{t0+k-1}
+  void* adj_lam[2] = {nullptr, nullptr};
+  double* adj_galpha = nullptr;
 };
 
 namespace {
@@ -126,7 +136,9 @@ int grid_1d(long long n) {
 int validate_common(const flb_lattice_desc* d) {
   if (!d) return fail(FLB_ERR_INVALID, "null descriptor");
   if (d->storage < 0 || d->storage > 2) return fail(FLB_ERR_INVALID, "bad storage %d", d->storage);
-  if (d->model < 0 || d->model > 2) return fail(FLB_ERR_INVALID, "bad model %d", d->model);
+  if (d->model < 0 || d->model > 3) return fail(FLB_ERR_INVALID, "bad model %d", d->model);
+  if (d->model == FLB_MODEL_BRINKMAN && d->storage == FLB_STORAGE_FP16S)
+    return fail(FLB_ERR_UNSUPPORTED, "BRINKMAN model is built for FP32 and FP64 storage");
   if (!(d->omega > 0.0 && d->omega < 2.0))
     return fail(FLB_ERR_INVALID, "omega %g outside (0, 2)", d->omega);
   if (d->ntasks < 0 || d->ntasks > FLB_MAX_TASKS)
@@ -159,6 +171,7 @@ void build_params(flb_lattice* h) {
   p.flags = h->flags;
   p.rho = h->rho;
   p.vel = h->vel;
+  p.alpha = h->alpha;
   p.nx = b0.L.nx;
   p.ny = b0.L.ny;
   p.nz = b0.L.nz;
@@ -192,9 +205,21 @@ void build_params(flb_lattice* h) {
   p.inv_scale = 1.0f / 1024.0f;
 }
 
+// Cells per thread of the pull kernel (launch parameter; defaults are the
+// measured best per storage).
+int default_vec(int storage) { return storage == FLB_STORAGE_FP16S ? 4 : 2; }
+int vec_width(const flb_lattice* h) { return h->vec ? h->vec : default_vec(h->desc.storage); }
+bool vec_allowed(int storage, int v) {
+  return storage == FLB_STORAGE_FP64 ? (v == 1 || v == 2) : (v == 2 || v == 4);
+}
+
+Geom geom_of(const HostBlock& b) {
+  return Geom{b.L.nx, b.L.ny, b.L.nz, b.L.pitch, b.L.plane, b.base};
+}
+
 // Block table for the tile kernel (rebuilt when tile_y changes).
 int upload_block_table(flb_lattice* h) {
-  if (h->d_blocks && h->table_tile_y == h->tile_y) return FLB_OK;
+  if (h->d_blocks && h->table_tile_y == h->tile_y && h->table_vec == vec_width(h)) return FLB_OK;
   std::vector<BlockEntry> t(h->blocks.size());
   long long start = 0;
   for (size_t b = 0; b < h->blocks.size(); ++b) {
@@ -202,17 +227,27 @@ int upload_block_table(flb_lattice* h) {
     BlockEntry& e = t[b];
     e.g = Geom{hb.L.nx, hb.L.ny, hb.L.nz, hb.L.pitch, hb.L.plane, hb.base};
     e.omega = hb.omega;
-    e.tiles_x = hb.L.pitch / 32;
-    e.tiles_y = (hb.L.ny + h->tile_y - 1) / h->tile_y;
+    const long long chunks = (long long)(hb.L.pitch / vec_width(h)) * hb.L.ny * hb.L.nz;
+    const long long per_tile = 32LL * h->tile_y;
     e.tile_start = start;
-    start += (long long)e.tiles_x * e.tiles_y * hb.L.nz;
+    start += (chunks + per_tile - 1) / per_tile;
   }
   if (!h->d_blocks) FLB_CUDA(cudaMalloc((void**)&h->d_blocks, t.size() * sizeof(BlockEntry)));
   FLB_CUDA(cudaMemcpy(h->d_blocks, t.data(), t.size() * sizeof(BlockEntry),
                       cudaMemcpyHostToDevice));
   h->ntiles = start;
   h->table_tile_y = h->tile_y;
+  h->table_vec = vec_width(h);
   return FLB_OK;
+}
+
+// Host twin of wrap_src (flb_pull.cuh): P slot feeding R_i at (x,y,z).
+long long host_wrap_src(const Geom& g, int x, int y, int z, int i) {
+  int sx = x - cx(i), sy = y - cy(i), sz = z - cz(i);
+  if (sx < 0) { sx += g.nx; --sy; } else if (sx >= g.nx) { sx -= g.nx; ++sy; }
+  if (sy < 0) { sy += g.ny; --sz; } else if (sy >= g.ny) { sy -= g.ny; ++sz; }
+  if (sz < 0) sz += g.nz; else if (sz >= g.nz) sz -= g.nz;
+  return g.base + sx + (long long)sy * g.pitch + (long long)sz * g.plane;
 }
 
 // Halo records: every overlap cell of block b owned by a neighbour's interior
@@ -241,9 +276,10 @@ int build_halo(flb_lattice* h) {
           o = k;
         }
   }
-  std::vector<HaloRec> recs;
+  std::vector<HaloCopy> recs;
   for (int k = 0; k < nb; ++k) {
     const HostBlock& b = h->blocks[k];
+    const Geom gb = geom_of(b);
     for (int lz = 0; lz < b.L.nz; ++lz)
       for (int ly = 0; ly < b.L.ny; ++ly)
         for (int lx = 0; lx < b.L.nx; ++lx) {
@@ -254,27 +290,27 @@ int build_halo(flb_lattice* h) {
           const int o = owner[size_t((long long)(z * (long long)gy + y) * gx + x)];
           if (o < 0) continue;
           const HostBlock& n = h->blocks[o];
-          unsigned mask = 0;
+          const Geom gn = geom_of(n);
+          const int l[3] = {lx, ly, lz};
+          const int m[3] = {b.L.nx, b.L.ny, b.L.nz};
           for (int i = 1; i < Q; ++i) {
             const int c[3] = {cx(i), cy(i), cz(i)};
-            const int l[3] = {lx, ly, lz};
-            const int m[3] = {b.L.nx, b.L.ny, b.L.nz};
-            for (int a = 0; a < 3; ++a) {
-              if ((l[a] == 0 && c[a] > 0) || (l[a] == m[a] - 1 && c[a] < 0)) mask |= 1u << i;
-            }
+            bool cross = false;
+            for (int a = 0; a < 3; ++a)
+              if ((l[a] == 0 && c[a] > 0) || (l[a] == m[a] - 1 && c[a] < 0)) cross = true;
+            if (!cross) continue;
+            HaloCopy r;
+            r.dir = i;
+            r.dst = host_wrap_src(gb, lx, ly, lz, i);
+            r.src = host_wrap_src(gn, x - n.ox, y - n.oy, z - n.oz, i);
+            recs.push_back(r);
           }
-          HaloRec r;
-          r.dst = b.base + lx + (long long)ly * b.L.pitch + (long long)lz * b.L.plane;
-          const int nx_ = x - n.ox, ny_ = y - n.oy, nz_ = z - n.oz;
-          r.src = n.base + nx_ + (long long)ny_ * n.L.pitch + (long long)nz_ * n.L.plane;
-          r.mask = mask;
-          recs.push_back(r);
         }
   }
   h->nhalo = (long long)recs.size();
   if (!recs.empty()) {
-    FLB_CUDA(cudaMalloc((void**)&h->d_halo, recs.size() * sizeof(HaloRec)));
-    FLB_CUDA(cudaMemcpy(h->d_halo, recs.data(), recs.size() * sizeof(HaloRec),
+    FLB_CUDA(cudaMalloc((void**)&h->d_halo, recs.size() * sizeof(HaloCopy)));
+    FLB_CUDA(cudaMemcpy(h->d_halo, recs.data(), recs.size() * sizeof(HaloCopy),
                         cudaMemcpyHostToDevice));
   }
   return FLB_OK;
@@ -290,23 +326,36 @@ int with_types(flb_lattice* h, F&& f) {
   }
 }
 
-template <typename S, typename R, int MODEL>
-void launch_one_step(flb_lattice* h, cudaStream_t st) {
+template <typename S, typename R, int MODEL, int V>
+void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
   const bool single = h->mode < 0 && h->ctas_per_sm == 0;
-  const dim3 block(32, h->tile_y);
   if (single) {
     const HostBlock& b = h->blocks[0];
-    const dim3 grid(b.L.pitch / 32, (b.L.ny + h->tile_y - 1) / h->tile_y, b.L.nz);
-    k_stream_collide<S, R, MODEL><<<grid, block, 0, st>>>(h->sp);
+    const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
+    const long long per_cta = 32LL * h->tile_y;
+    const dim3 grid(unsigned((chunks + per_cta - 1) / per_cta));
+    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(h->sp);
   } else {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));
-    k_stream_collide_blocks<S, R, MODEL><<<unsigned(g), block, 0, st>>>(
+    k_pull_blocks<S, R, MODEL, V><<<unsigned(g), dim3(32 * h->tile_y), 0, st>>>(
         h->sp, h->d_blocks, int(h->blocks.size()), h->ntiles);
   }
+}
+
+template <typename S, typename R, int MODEL>
+void launch_one_step(flb_lattice* h, cudaStream_t st) {
+  const int v = vec_width(h);
+  if constexpr (std::is_same<S, double>::value) {
+    if (v == 1) launch_one_step_v<S, R, MODEL, 1>(h, st);
+    else launch_one_step_v<S, R, MODEL, 2>(h, st);
+  } else {
+    if (v == 2) launch_one_step_v<S, R, MODEL, 2>(h, st);
+    else launch_one_step_v<S, R, MODEL, 4>(h, st);
+  }
   if (h->nhalo > 0)
-    k_halo<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, int(h->nhalo),
-                                                 static_cast<S*>(h->sp.dst), h->dstride);
+    k_halo_pull<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, h->nhalo,
+                                                      static_cast<S*>(h->sp.dst), h->dstride);
 }
 
 template <typename S, typename R>
@@ -318,10 +367,42 @@ int launch_steps(flb_lattice* h, int nsteps, cudaStream_t st) {
     switch (h->desc.model) {
       case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
       case FLB_MODEL_MRT: launch_one_step<S, R, MODEL_MRT>(h, st); break;
-      default: launch_one_step<S, R, MODEL_LES>(h, st); break;
+      case FLB_MODEL_LES: launch_one_step<S, R, MODEL_LES>(h, st); break;
+      default:
+        if constexpr (!std::is_same<S, __half>::value)
+          launch_one_step<S, R, MODEL_BRINKMAN>(h, st);
+        break;
     }
     h->cur ^= 1;
   }
+  FLB_CUDA(cudaGetLastError());
+  return FLB_OK;
+}
+
+// One step from buffer src into buffer dst (adjoint recompute), leaving the
+// handle's own ping-pong state untouched.
+int step_between(flb_lattice* h, const void* src, void* dst, cudaStream_t st) {
+  const void* s0 = h->sp.src;
+  void* d0 = h->sp.dst;
+  h->sp.src = src;
+  h->sp.dst = dst;
+  int rc = with_types(h, [&](auto* sp, auto* rp) {
+    using S = std::remove_pointer_t<decltype(sp)>;
+    using R = std::remove_pointer_t<decltype(rp)>;
+    switch (h->desc.model) {
+      case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
+      case FLB_MODEL_MRT: launch_one_step<S, R, MODEL_MRT>(h, st); break;
+      case FLB_MODEL_LES: launch_one_step<S, R, MODEL_LES>(h, st); break;
+      default:
+        if constexpr (!std::is_same<S, __half>::value)
+          launch_one_step<S, R, MODEL_BRINKMAN>(h, st);
+        break;
+    }
+    return FLB_OK;
+  });
+  h->sp.src = s0;
+  h->sp.dst = d0;
+  if (rc) return rc;
   FLB_CUDA(cudaGetLastError());
   return FLB_OK;
 }
@@ -346,25 +427,22 @@ int pops_transfer(flb_lattice* h, const HostBlock& B, void* host, bool upload, c
   const LayoutParams& L = B.L;
   const size_t hb = sizeof(H);
   const size_t N = size_t(L.nx) * L.ny * L.nz;
-  const bool direct = std::is_same<S, H>::value;
-  if (!direct) FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
-  S* pops = static_cast<S*>(h->pops[h->cur]) + B.base;
+  FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
+  S* pops = static_cast<S*>(h->pops[h->cur]);
+  const Geom g = geom_of(B);
   for (int i = 0; i < Q; ++i) {
     char* hp = static_cast<char*>(host) + i * N * hb;
-    void* dev = direct ? static_cast<void*>(pops + i * h->dstride) : h->stage;
     if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, hp, L.nx * hb, L.nx * hb,
+      FLB_CUDA(cudaMemcpy2DAsync(h->stage, L.pitch * hb, hp, L.nx * hb, L.nx * hb,
                                  size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      if (!direct)
-        k_pops_in<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
-            L, static_cast<const H*>(h->stage), pops + i * h->dstride, h->sp.shift[i],
-            h->sp.scale);
+      k_unstream_in<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
+          L, g, static_cast<const H*>(h->stage), pops + i * h->dstride, i, h->sp.shift[i],
+          h->sp.scale);
     } else {
-      if (!direct)
-        k_pops_out<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
-            L, static_cast<H*>(h->stage), pops + i * h->dstride, h->sp.shift[i],
-            h->sp.inv_scale);
-      FLB_CUDA(cudaMemcpy2DAsync(hp, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
+      k_stream_out<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
+          L, g, static_cast<H*>(h->stage), pops + i * h->dstride, i, h->sp.shift[i],
+          h->sp.inv_scale);
+      FLB_CUDA(cudaMemcpy2DAsync(hp, L.nx * hb, h->stage, L.pitch * hb, L.nx * hb,
                                  size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
     }
     FLB_CUDA(cudaGetLastError());
@@ -393,9 +471,11 @@ int field_transfer(flb_lattice* h, const HostBlock& B, int field, void* host, bo
                    cudaStream_t st) {
   const LayoutParams& L = B.L;
   const size_t hb = sizeof(H);
-  R* rho = static_cast<R*>(h->rho) + B.base;
+  R* rho = static_cast<R*>(field == FLB_FIELD_ALPHA ? h->alpha : h->rho) + B.base;
   R* vel = static_cast<R*>(h->vel) + B.base;
-  if (field == FLB_FIELD_RHO) {
+  if (field == FLB_FIELD_ALPHA && !h->alpha)
+    return fail(FLB_ERR_STATE, "no ALPHA field: the lattice model is not BRINKMAN");
+  if (field == FLB_FIELD_RHO || field == FLB_FIELD_ALPHA) {
     const bool direct = std::is_same<R, H>::value;
     if (!direct) FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
     void* dev = direct ? static_cast<void*>(rho) : h->stage;
@@ -485,7 +565,7 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
   h->real_bytes = desc->storage == FLB_STORAGE_FP64 ? 8 : 4;
   long long off = 0;
   for (HostBlock& b : blocks) {
-    b.L.pitch = (b.L.nx + 31) / 32 * 32;
+    b.L.pitch = (b.L.nx + 15) / 16 * 16;
     b.L.plane = (long long)b.L.pitch * b.L.ny;
     b.base = off;
     off += (b.padded() + 63) / 64 * 64;
@@ -505,6 +585,11 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
       (e = cudaMalloc(&h->vel, 3 * ds * h->real_bytes)) != cudaSuccess ||
       (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess)
     return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
+  if (desc->model == FLB_MODEL_BRINKMAN) {
+    if ((e = cudaMalloc(&h->alpha, ds * h->real_bytes)) != cudaSuccess ||
+        (e = cudaMemset(h->alpha, 0, ds * h->real_bytes)) != cudaSuccess)
+      return cleanup(fail(FLB_ERR_OOM, "cudaMalloc alpha: %s", cudaGetErrorString(e)));
+  }
   build_params(h);
   if (mode == FLB_BLOCKS_HALO) {
     int rc = build_halo(h);
@@ -615,10 +700,35 @@ int flb_create_blocks(const flb_lattice_desc* desc, int nblocks, const flb_block
 int flb_destroy(flb_lattice* h) {
   if (!h) return FLB_OK;
   drop_graphs(h);
+  flb_adjoint_release(h);
+  if (h->alpha) cudaFree(h->alpha);
   for (void* p : {h->pops[0], h->pops[1], (void*)h->flags, h->rho, h->vel, (void*)h->acc,
                   h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo})
     if (p) cudaFree(p);
   delete h;
+  return FLB_OK;
+}
+
+int flb_set_tasks(flb_lattice* h, int ntasks, const uint8_t* keys, const uint8_t* ops, int model) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (ntasks < 0 || ntasks > FLB_MAX_TASKS || (ntasks > 0 && (!keys || !ops)))
+    return fail(FLB_ERR_INVALID, "ntasks %d outside [0, %d] or null lists", ntasks, FLB_MAX_TASKS);
+  flb_lattice_desc d = h->desc;
+  d.ntasks = ntasks;
+  for (int t = 0; t < ntasks; ++t) {
+    d.task_keys[t] = keys[t];
+    d.task_ops[t] = ops[t];
+  }
+  d.model = model;
+  FLB_TRY(validate_common(&d));
+  if (model == FLB_MODEL_BRINKMAN && !h->alpha)
+    return fail(FLB_ERR_STATE, "BRINKMAN needs the ALPHA field: create the lattice with it");
+  h->desc = d;
+  const StepParams keep = h->sp;
+  build_params(h);
+  h->sp.src = keep.src;
+  h->sp.dst = keep.dst;
+  drop_graphs(h);
   return FLB_OK;
 }
 
@@ -639,7 +749,7 @@ int flb_memory_bytes(const flb_lattice* h, size_t* bytes) {
   const size_t ds = size_t(h->dstride);
   *bytes = 2 * size_t(Q) * ds * h->elem_bytes + ds + 4 * ds * h->real_bytes + 64 +
            h->stage_bytes + (h->uprev ? 3 * ds * sizeof(double) : 0) +
-           h->blocks.size() * sizeof(BlockEntry) + size_t(h->nhalo) * sizeof(HaloRec);
+           h->blocks.size() * sizeof(BlockEntry) + size_t(h->nhalo) * sizeof(HaloCopy);
   return FLB_OK;
 }
 
@@ -739,67 +849,79 @@ int flb_step_graph(flb_lattice* h, int nsteps, void* stream) {
   return FLB_OK;
 }
 
-int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm) {
+int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_thread) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (cells_per_thread != 0 && !vec_allowed(h->desc.storage, cells_per_thread))
+    return fail(FLB_ERR_INVALID, "cells_per_thread %d not built for this storage",
+                cells_per_thread);
   if (tile_y != 1 && tile_y != 2 && tile_y != 4 && tile_y != 8)
     return fail(FLB_ERR_INVALID, "tile_y %d not in {1,2,4,8}", tile_y);
   if (ctas_per_sm < 0 || ctas_per_sm > 32)
     return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [0, 32]", ctas_per_sm);
-  if (tile_y != h->tile_y || ctas_per_sm != h->ctas_per_sm) drop_graphs(h);
+  const int v = cells_per_thread ? cells_per_thread : default_vec(h->desc.storage);
+  if (tile_y != h->tile_y || ctas_per_sm != h->ctas_per_sm || v != vec_width(h)) drop_graphs(h);
   h->tile_y = tile_y;
   h->ctas_per_sm = ctas_per_sm;
+  h->vec = v;
   return FLB_OK;
 }
 
-int flb_get_launch(const flb_lattice* h, int* tile_y, int* ctas_per_sm) {
+int flb_get_launch(const flb_lattice* h, int* tile_y, int* ctas_per_sm, int* cells_per_thread) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   if (tile_y) *tile_y = h->tile_y;
   if (ctas_per_sm) *ctas_per_sm = h->ctas_per_sm;
+  if (cells_per_thread) *cells_per_thread = vec_width(h);
   return FLB_OK;
 }
 
 int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int* ctas_per_sm,
-                 double* best_ms, int* steps_taken) {
+                 int* cells_per_thread, double* best_ms, int* steps_taken) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   if (trial_steps < 1) return fail(FLB_ERR_INVALID, "trial_steps %d < 1", trial_steps);
   cudaStream_t st = as_stream(stream);
   const int tys[] = {1, 2, 4, 8};
-  const int ctas[] = {0, 2, 4, 8};
-  const int ty0 = h->tile_y, c0 = h->ctas_per_sm;
-  int best_ty = ty0, best_c = c0, taken = 0;
+  const int ctas[] = {0, 8, 16, 32};
+  const int vecs_d[] = {1, 2}, vecs_f[] = {2, 4};
+  const int* vecs = h->desc.storage == FLB_STORAGE_FP64 ? vecs_d : vecs_f;
+  const int ty0 = h->tile_y, c0 = h->ctas_per_sm, v0 = vec_width(h);
+  int best_ty = ty0, best_c = c0, best_v = v0, taken = 0;
   float best = 1e30f;
   cudaEvent_t e0, e1;
   FLB_CUDA(cudaEventCreate(&e0));
   FLB_CUDA(cudaEventCreate(&e1));
   int rc = FLB_OK;
-  for (int ty : tys) {
-    for (int c : ctas) {
-      if ((rc = flb_set_launch(h, ty, c))) break;
-      if ((rc = step_any(h, 1, st))) break;  // warm-up (block table upload, caches)
-      cudaEventRecord(e0, st);
-      if ((rc = step_any(h, trial_steps, st))) break;
-      cudaEventRecord(e1, st);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      taken += trial_steps + 1;
-      if (ms < best) {
-        best = ms;
-        best_ty = ty;
-        best_c = c;
+  for (int vi = 0; vi < 2 && !rc; ++vi) {
+    for (int ty : tys) {
+      for (int c : ctas) {
+        if ((rc = flb_set_launch(h, ty, c, vecs[vi]))) break;
+        if ((rc = step_any(h, 1, st))) break;  // warm-up (block table upload, caches)
+        cudaEventRecord(e0, st);
+        if ((rc = step_any(h, trial_steps, st))) break;
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        taken += trial_steps + 1;
+        if (ms < best) {
+          best = ms;
+          best_ty = ty;
+          best_c = c;
+          best_v = vecs[vi];
+        }
       }
+      if (rc) break;
     }
-    if (rc) break;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) {
-    flb_set_launch(h, ty0, c0);
+    flb_set_launch(h, ty0, c0, v0);
     return rc;
   }
-  FLB_TRY(flb_set_launch(h, best_ty, best_c));
+  FLB_TRY(flb_set_launch(h, best_ty, best_c, best_v));
   if (tile_y) *tile_y = best_ty;
   if (ctas_per_sm) *ctas_per_sm = best_c;
+  if (cells_per_thread) *cells_per_thread = best_v;
   if (best_ms) *best_ms = double(best) / trial_steps;
   if (steps_taken) *steps_taken = taken;
   return FLB_OK;
@@ -812,9 +934,9 @@ int flb_compute_rhou(flb_lattice* h, uint8_t key, void* stream) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
     return for_blocks(h, [&](const HostBlock& b) {
-      k_rhou<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key,
-          static_cast<R*>(h->rho) + b.base, static_cast<R*>(h->vel) + b.base, h->sp);
+      k_rhou_pull<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->flags, key,
+          static_cast<R*>(h->rho), static_cast<R*>(h->vel), h->sp);
       return FLB_OK;
     });
   }));
@@ -830,8 +952,8 @@ int flb_reduce_conservation(flb_lattice* h, uint8_t key, double out[4], void* st
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
     return for_blocks(h, [&](const HostBlock& b) {
-      k_conservation<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key, h->acc,
+      k_conservation_pull<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->acc,
           h->sp);
       return FLB_OK;
     });
@@ -855,9 +977,9 @@ int flb_tolerance_u(flb_lattice* h, uint8_t key, double* max_du, void* stream) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
     return for_blocks(h, [&](const HostBlock& b) {
-      k_tolerance<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, key,
-          h->uprev + b.base, acc, h->sp);
+      k_tolerance_pull<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->uprev,
+          acc, h->sp);
       return FLB_OK;
     });
   }));
@@ -911,6 +1033,178 @@ int flb_device_pointers(flb_lattice* h, void** pops, void** flags, void** rho, v
   if (rho) *rho = h->rho;
   if (vel) *vel = h->vel;
   return FLB_OK;
+}
+
+int flb_objective_u2(flb_lattice* h, double* J, void* stream) {
+  if (!h || !J) return fail(FLB_ERR_INVALID, "null argument");
+  if (h->blocks.size() != 1) return fail(FLB_ERR_UNSUPPORTED, "objective on single-block handles");
+  if (h->desc.storage == FLB_STORAGE_FP16S)
+    return fail(FLB_ERR_UNSUPPORTED, "objective is built for FP32 and FP64 storage");
+  cudaStream_t st = as_stream(stream);
+  double* jacc = h->acc + 4;
+  FLB_CUDA(cudaMemsetAsync(jacc, 0, sizeof(double), st));
+  const HostBlock& b = h->blocks[0];
+  int rc = with_types(h, [&](auto* sp, auto* rp) {
+    using S = std::remove_pointer_t<decltype(sp)>;
+    using R = std::remove_pointer_t<decltype(rp)>;
+    if constexpr (!std::is_same<S, __half>::value)
+      k_objective<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->sp, (R*)nullptr,
+          (double*)nullptr, jacc, false);
+    return FLB_OK;
+  });
+  if (rc) return rc;
+  FLB_CUDA(cudaGetLastError());
+  FLB_CUDA(cudaMemcpyAsync(J, jacc, sizeof(double), cudaMemcpyDeviceToHost, st));
+  FLB_CUDA(cudaStreamSynchronize(st));
+  return FLB_OK;
+}
+
+int flb_adjoint_release(flb_lattice* h) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  for (void* p : h->adj_ckpt) cudaFree(p);
+  for (void* p : h->adj_seg) cudaFree(p);
+  h->adj_ckpt.clear();
+  h->adj_seg.clear();
+  for (auto& p : h->adj_lam)
+    if (p) {
+      cudaFree(p);
+      p = nullptr;
+    }
+  if (h->adj_galpha) cudaFree(h->adj_galpha);
+  h->adj_galpha = nullptr;
+  h->adj_T = h->adj_k = 0;
+  return FLB_OK;
+}
+
+static int adjoint_supported(flb_lattice* h) {
+  if (h->blocks.size() != 1 || h->mode >= 0)
+    return fail(FLB_ERR_UNSUPPORTED, "the adjoint runs on single-block handles");
+  if (h->desc.storage == FLB_STORAGE_FP16S)
+    return fail(FLB_ERR_UNSUPPORTED, "the adjoint is built for FP32 and FP64 storage");
+  if (h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_BRINKMAN)
+    return fail(FLB_ERR_UNSUPPORTED, "the adjoint covers BGK and BRINKMAN bulk models");
+  for (int t = 0; t < h->desc.ntasks; ++t)
+    if (h->desc.task_ops[t] == FLB_OP_FIELD_BGK)
+      return fail(FLB_ERR_UNSUPPORTED, "the adjoint does not cover FIELD_BGK cells");
+  return FLB_OK;
+}
+
+int flb_adjoint_forward(flb_lattice* h, int nsteps, int every, double* J, void* stream) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  FLB_TRY(adjoint_supported(h));
+  if (nsteps < 1 || every < 1) return fail(FLB_ERR_INVALID, "nsteps and checkpoint_every >= 1");
+  cudaStream_t st = as_stream(stream);
+  flb_adjoint_release(h);
+  const size_t bytes = size_t(Q) * size_t(h->dstride) * h->elem_bytes;
+  const int nck = (nsteps + every - 1) / every;
+  for (int c = 0; c < nck; ++c) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      flb_adjoint_release(h);
+      return fail(FLB_ERR_OOM, "checkpoint %d of %d (%zu bytes): %s", c, nck, bytes,
+                  cudaGetErrorString(e));
+    }
+    h->adj_ckpt.push_back(p);
+  }
+  h->adj_T = nsteps;
+  h->adj_k = every;
+  for (int t = 0; t < nsteps; ++t) {
+    if (t % every == 0)
+      FLB_CUDA(cudaMemcpyAsync(h->adj_ckpt[t / every], h->pops[h->cur], bytes,
+                               cudaMemcpyDeviceToDevice, st));
+    FLB_TRY(step_any(h, 1, st));
+  }
+  if (J) FLB_TRY(flb_objective_u2(h, J, stream));
+  return FLB_OK;
+}
+
+}  // extern "C"
+
+template <typename R>
+static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau,
+                              double* dJ_dulid, cudaStream_t st) {
+  constexpr int V = std::is_same<R, double>::value ? 1 : 2;
+  const HostBlock& b = h->blocks[0];
+  const size_t ds = size_t(h->dstride);
+  const size_t qbytes = size_t(Q) * ds * h->elem_bytes;
+  const size_t lbytes = size_t(Q) * ds * sizeof(R);
+  for (auto& p : h->adj_lam)
+    if (!p) FLB_CUDA(cudaMalloc(&p, lbytes));
+  if (!h->adj_galpha) FLB_CUDA(cudaMalloc((void**)&h->adj_galpha, ds * sizeof(double)));
+  FLB_CUDA(cudaMemsetAsync(h->adj_galpha, 0, ds * sizeof(double), st));
+  const int k = h->adj_k;
+  while ((int)h->adj_seg.size() < k - 1) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, qbytes);
+    if (e != cudaSuccess)
+      return fail(FLB_ERR_OOM, "recompute slot (%zu bytes): %s", qbytes, cudaGetErrorString(e));
+    h->adj_seg.push_back(p);
+  }
+  double* gscal = h->acc + 5;  // [0] tau, [1] u_lid
+  double* jacc = h->acc + 4;
+  FLB_CUDA(cudaMemsetAsync(h->acc + 4, 0, 3 * sizeof(double), st));
+  // seed lambda_T = dJ/dR_T and the direct dJ/dalpha term
+  k_objective<R, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+      b.L, geom_of(b), static_cast<const R*>(h->pops[h->cur]), h->sp,
+      static_cast<R*>(h->adj_lam[0]), h->alpha ? h->adj_galpha : nullptr, jacc, true);
+  FLB_CUDA(cudaGetLastError());
+  int cur = 0;
+  const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
+  const dim3 block(32 * h->tile_y);
+  const dim3 grid(unsigned((chunks + block.x - 1) / block.x));
+  AdjParams a{};
+  a.galpha = h->adj_galpha;
+  a.gscal = gscal;
+  const int T = h->adj_T;
+  const int nseg = (T + k - 1) / k;
+  for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+    const int t0 = sgi * k, t1 = std::min(T, t0 + k);
+    // states Q_t0 .. Q_{t1-1}: slot 0 is the checkpoint, the rest recomputed
+    std::vector<const void*> q(t1 - t0);
+    q[0] = h->adj_ckpt[sgi];
+    for (int t = t0 + 1; t < t1; ++t) {
+      FLB_TRY(step_between(h, q[t - 1 - t0], h->adj_seg[t - 1 - t0], st));
+      q[t - t0] = h->adj_seg[t - 1 - t0];
+    }
+    for (int t = t1 - 1; t >= t0; --t) {
+      a.lam_in = h->adj_lam[cur];
+      a.lam_out = h->adj_lam[cur ^ 1];
+      a.q = q[t - t0];
+      k_adjoint_step<R, V><<<grid, block, 0, st>>>(h->sp, a);
+      cur ^= 1;
+    }
+    FLB_CUDA(cudaGetLastError());
+  }
+  double sc[2] = {0, 0};
+  FLB_CUDA(cudaMemcpyAsync(sc, gscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (dJ_dalpha) {
+    const LayoutParams& L = b.L;
+    FLB_CUDA(cudaMemcpy2DAsync(dJ_dalpha, L.nx * sizeof(double), h->adj_galpha,
+                               L.pitch * sizeof(double), L.nx * sizeof(double),
+                               size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+  }
+  FLB_CUDA(cudaStreamSynchronize(st));
+  if (dJ_dtau) *dJ_dtau = sc[0];
+  if (dJ_dulid) *dJ_dulid = sc[1];
+  return FLB_OK;
+}
+
+extern "C" {
+
+int flb_adjoint_backward(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau, double* dJ_dulid,
+                         void* stream) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  FLB_TRY(adjoint_supported(h));
+  if (h->adj_T < 1 || h->adj_ckpt.empty())
+    return fail(FLB_ERR_STATE, "flb_adjoint_backward needs a preceding flb_adjoint_forward");
+  if (dJ_dalpha && !h->alpha)
+    return fail(FLB_ERR_STATE, "dJ/dalpha needs the BRINKMAN model (ALPHA field)");
+  cudaStream_t st = as_stream(stream);
+  if (h->desc.storage == FLB_STORAGE_FP64)
+    return adjoint_backward_t<double>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
+  return adjoint_backward_t<float>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
 }
 
 }  // extern "C"

@@ -171,6 +171,53 @@ __device__ __forceinline__ void bgk(R* f, R omega, R omega_c) {
   for (int i = 0; i < Q; ++i) f[i] = omega * feq[i] + omega_c * f[i];
 }
 
+// Brinkman drag F = -alpha u through the reference's Guo forcing:
+// moment::forcerhoU (src/lbm/moment.h:402-422) gives u = (sum c f + F/2)/rho,
+// which with F = -alpha u is u = sum c f / (rho + alpha/2); force::ForcePopImpl
+// (src/lbm/force.h:29-36) gives F_i = w_i F.(3 (c_i - u) + 9 (c_i.u) c_i);
+// collision::BGKForce (src/lbm/collision.h:61-90) relaxes
+// f <- omega feq + (1-omega) f + (1 - omega/2) F_i.
+template <typename R>
+__device__ __forceinline__ void bgk_brinkman(R* f, R omega, R alpha) {
+  const R rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] +
+                f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+  const R mx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16];
+  const R my = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18];
+  const R mz = f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18];
+  const R den = rho + R(0.5) * alpha;
+  const R ux = mx / den, uy = my / den, uz = mz / den;
+  const R Fx = -alpha * ux, Fy = -alpha * uy, Fz = -alpha * uz;
+  R feq[Q];
+  feq2(feq, rho, ux, uy, uz);
+  const R fomega = R(1) - R(0.5) * omega;
+  const R omega_c = R(1) - omega;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const R cu = R(cx(i)) * ux + R(cy(i)) * uy + R(cz(i)) * uz;
+    const R vx = (R(cx(i)) - ux) * R(3) + cu * R(9) * R(cx(i));
+    const R vy = (R(cy(i)) - uy) * R(3) + cu * R(9) * R(cy(i));
+    const R vz = (R(cz(i)) - uz) * R(3) + cu * R(9) * R(cz(i));
+    const R Fi = weight<R>(i) * (Fx * vx + Fy * vy + Fz * vz);
+    f[i] = omega * feq[i] + omega_c * f[i] + fomega * Fi;
+  }
+}
+
+// Forced moments of a Brinkman cell: rho = sum f, u = sum c f / (rho + alpha/2)
+// (moment::forcerhoU with F = -alpha u, src/lbm/moment.h:402-422).
+template <typename R>
+__device__ __forceinline__ void forced_moments(const R* f, R alpha, R& rho, R& den, R& ux, R& uy,
+                                               R& uz) {
+  rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8] + f[9] + f[10] + f[11] +
+        f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18];
+  const R mx = f[1] - f[2] + f[7] - f[8] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16];
+  const R my = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] - f[13] + f[14] + f[17] - f[18];
+  const R mz = f[5] - f[6] + f[9] - f[10] + f[11] - f[12] - f[15] + f[16] - f[17] + f[18];
+  den = rho + R(0.5) * alpha;
+  ux = mx / den;
+  uy = my / den;
+  uz = mz / den;
+}
+
 // collision::BGK<moment::useFieldrhoU, ...>: rho, u from the fields.
 template <typename R>
 __device__ __forceinline__ void bgk_field(R* f, R omega, R omega_c, R rho, R ux, R uy, R uz) {

@@ -59,6 +59,7 @@ extern "C" {
 #define FLB_MODEL_BGK 0 /* collision::BGK<moment::rhoU, equilibrium::SecondOrder> */
 #define FLB_MODEL_MRT 1 /* collision::MRT_Feq_RhoU, D3Q19 Gram-Schmidt basis */
 #define FLB_MODEL_LES 2 /* collision::SmagorinskyBGK<moment::rhoU<CELL,true>, ...> */
+#define FLB_MODEL_BRINKMAN 3 /* collision::BGKForce with Guo drag F = -alpha u (ALPHA field) */
 
 /* per-flag operations (the policy of a tmp::Key_TypePair) */
 #define FLB_OP_NONE 0       /* no collision (void cells) */
@@ -74,6 +75,7 @@ extern "C" {
 /* fields */
 #define FLB_FIELD_RHO 0      /* RHO<T>: N values */
 #define FLB_FIELD_VELOCITY 1 /* VELOCITY<T,3>: N x 3 values, AoS like Vector<T,3> */
+#define FLB_FIELD_ALPHA 2    /* Brinkman porosity alpha (FLB_MODEL_BRINKMAN): N values */
 
 #define FLB_MAX_TASKS 8
 
@@ -141,6 +143,12 @@ FLB_API int flb_create_blocks(const flb_lattice_desc* desc, int nblocks,
 FLB_API int flb_block_count(const flb_lattice* lat, int* nblocks);
 /* number of halo copy records (overlap cells fed by a neighbour) */
 FLB_API int flb_halo_count(const flb_lattice* lat, long long* nrecords);
+
+/* Rebind the per-flag task list and the bulk model (the NSTask type of
+ * ApplyCellDynamics<NSTask>, src/utils/tmp.h:283-309): tasks are tried in order,
+ * a cell takes the op of the first task whose key shares a bit with its flag. */
+FLB_API int flb_set_tasks(flb_lattice* lat, int ntasks, const uint8_t* keys, const uint8_t* ops,
+                          int model);
 
 /* Device bytes held by the handle. */
 FLB_API int flb_memory_bytes(const flb_lattice* lat, size_t* bytes);
@@ -216,22 +224,47 @@ FLB_API int flb_upload_field_block(flb_lattice* lat, int block, int field, const
 FLB_API int flb_download_field_block(flb_lattice* lat, int block, int field, void* host,
                                      int host_dtype, void* stream);
 
-/* Launch shape of the stream-collide kernel: tile_y rows of 32 cells per CTA
- * (1, 2, 4 or 8) and ctas_per_sm resident CTAs per SM for a persistent grid
- * over the tile work table (0 = one CTA per tile). */
-FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm);
-FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm);
+/* Launch shape of the stream-collide kernel: tile_y warps (rows) per CTA
+ * (1, 2, 4 or 8), ctas_per_sm CTAs per SM for a persistent grid over the tile
+ * work table (0 = one CTA per tile), and cells_per_thread (2 or 4 for FP32
+ * and FP16S, 1 or 2 for FP64; 0 = default 2 / 4 / 2).  Defaults: tile_y 4, no
+ * persistent grid. */
+FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm, int cells_per_thread);
+FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm,
+                           int* cells_per_thread);
 
 /* Autotuner: times every candidate launch shape for `trial_steps` steps on
  * `stream` (CUDA events) and keeps the fastest.  The trial steps are real
  * time steps: the lattice advances by *steps_taken.  best_ms = time per step
  * of the winner. */
 FLB_API int flb_autotune(flb_lattice* lat, int trial_steps, void* stream, int* tile_y,
-                         int* ctas_per_sm, double* best_ms, int* steps_taken);
+                         int* ctas_per_sm, int* cells_per_thread, double* best_ms,
+                         int* steps_taken);
 
 /* CUDA-graph stepping: the two-step ping-pong cycle (stream-collide, halo) is
  * captured once per handle and replayed; equivalent to flb_step. */
 FLB_API int flb_step_graph(flb_lattice* lat, int nsteps, void* stream);
+
+/* Objective J = sum over bulk cells of |u|^2 at the current state, with the
+ * forced moment u = sum c f / (rho + alpha/2) (alpha = 0 without a porosity
+ * field), reduced in FP64. */
+FLB_API int flb_objective_u2(flb_lattice* lat, double* J, void* stream);
+
+/* Discrete adjoint of the step (no reference counterpart: the reference has no
+ * differentiation).  Single-block handles, FP32 or FP64 storage, ops none /
+ * bulk (BGK or BRINKMAN) / bounce-back / moving wall.
+ * flb_adjoint_forward advances nsteps from the current state, keeping a copy of
+ * the state every `checkpoint_every` steps, and returns J at the end.
+ * flb_adjoint_backward returns dJ/dalpha (per cell, N doubles in reference
+ * order; may be NULL), dJ/dtau and dJ/du_lid (x-velocity of the moving-wall
+ * cells), accumulated in FP64; the states between checkpoints are recomputed.
+ * The lattice keeps the forward end state.  flb_adjoint_release frees the
+ * checkpoint and adjoint memory. */
+FLB_API int flb_adjoint_forward(flb_lattice* lat, int nsteps, int checkpoint_every, double* J,
+                                void* stream);
+FLB_API int flb_adjoint_backward(flb_lattice* lat, double* dJ_dalpha, double* dJ_dtau,
+                                 double* dJ_dulid, void* stream);
+FLB_API int flb_adjoint_release(flb_lattice* lat);
 
 #ifdef __cplusplus
 }

@@ -24,7 +24,7 @@ static const int ORC_C[19][3] = {
     {-1, 1, 0}, {1, 0, -1},  {-1, 0, 1}, {0, 1, -1},  {0, -1, 1}};
 
 enum { ORC_OP_NONE = 0, ORC_OP_BULK = 1, ORC_OP_BB = 2, ORC_OP_MBB = 3, ORC_OP_FIELD_BGK = 4 };
-enum { ORC_MODEL_BGK = 0, ORC_MODEL_MRT = 1, ORC_MODEL_LES = 2 };
+enum { ORC_MODEL_BGK = 0, ORC_MODEL_MRT = 1, ORC_MODEL_LES = 2, ORC_MODEL_BRINKMAN = 3 };
 
 typedef struct {
   int nx, ny, nz;       /* stored mesh, x fastest */
@@ -33,6 +33,7 @@ typedef struct {
   double cs_smag;       /* Smagorinsky constant (LES) */
   double mrt_s[19];     /* MRT rates; shear entries are replaced by omega */
   uint8_t op_lut[256];  /* op for each flag value (first matching task key) */
+  const void* alpha;    /* Brinkman porosity per cell (ORC_MODEL_BRINKMAN), OT[N] */
 } oracle_desc;
 
 /* D3Q19 d'Humieres 2002 basis on the reference ordering and its inverse

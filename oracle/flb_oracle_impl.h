@@ -140,6 +140,37 @@ static void FN(les)(OT* f, OT omega, OT cs, OT rho_field_unused) {
   FN(bgk_relax)(f, feq, eomega);
 }
 
+/* BGK with Brinkman drag F = -alpha u: the forced moment of
+ * moment::forcerhoUImpl (src/lbm/moment.h:408-422) solved for F = -alpha u,
+ * u = sum c f / (rho + alpha/2); force::ForcePop (src/lbm/force.h:29-36)
+ * F_i = (w_i F).(3 (c_i - u) + 9 (c_i.u) c_i); collision::BGKForce
+ * (src/lbm/collision.h:61-90) f <- omega feq + (1-omega) f + (1-omega/2) F_i. */
+static void FN(brinkman)(OT* f, OT omega, OT alpha) {
+  OT rho = 0, m[3] = {0, 0, 0}, u[3], F[3], feq[19];
+  for (int i = 0; i < 19; ++i) {
+    rho += f[i];
+    for (int d = 0; d < 3; ++d) m[d] += (OT)ORC_C[i][d] * f[i];
+  }
+  const OT den = rho + (OT)0.5 * alpha;
+  for (int d = 0; d < 3; ++d) {
+    u[d] = m[d] / den;
+    F[d] = u[d] * (-alpha);
+  }
+  FN(feq)(feq, rho, u);
+  const OT _omega = (OT)1 - omega;
+  const OT fomega = (OT)1 - (OT)0.5 * omega;
+  for (int i = 0; i < 19; ++i) {
+    const OT w = (i == 0) ? (OT)1 / (OT)3 : (i < 7 ? (OT)1 / (OT)18 : (OT)1 / (OT)36);
+    const OT cu = (OT)ORC_C[i][0] * u[0] + (OT)ORC_C[i][1] * u[1] + (OT)ORC_C[i][2] * u[2];
+    OT fi = 0;
+    for (int d = 0; d < 3; ++d) {
+      const OT v = ((OT)ORC_C[i][d] - u[d]) * (OT)3 + (cu * (OT)9) * (OT)ORC_C[i][d];
+      fi += (w * F[d]) * v;
+    }
+    f[i] = omega * feq[i] + _omega * f[i] + fomega * fi;
+  }
+}
+
 static void FN(mrt)(OT* f, OT omega, const double* M, const int* inv_num, const int* inv_den,
                     const double* s) {
   OT rho, u[3], feq[19], m[19], meq[19], rt[19];
@@ -193,6 +224,8 @@ int FN(oracle_step)(const oracle_desc* d, const uint8_t* flags, OT* pops, OT* tm
           FN(bgk_relax)(f, feq, omega);
         } else if (d->model == ORC_MODEL_LES) {
           FN(les)(f, omega, cs, 0);
+        } else if (d->model == ORC_MODEL_BRINKMAN) {
+          FN(brinkman)(f, omega, d->alpha ? ((const OT*)d->alpha)[id] : (OT)0);
         } else {
           FN(mrt)(f, omega, ORC_M, ORC_INV_NUM, ORC_INV_DEN, d->mrt_s);
         }

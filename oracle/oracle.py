@@ -21,7 +21,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 OP_NONE, OP_BULK, OP_BB, OP_MBB, OP_FIELD_BGK = 0, 1, 2, 3, 4
 MODEL_BGK, MODEL_MRT, MODEL_LES = 0, 1, 2
-MODELS = {"bgk": MODEL_BGK, "mrt": MODEL_MRT, "les": MODEL_LES}
+MODEL_BRINKMAN = 3
+MODELS = {"bgk": MODEL_BGK, "mrt": MODEL_MRT, "les": MODEL_LES, "brinkman": MODEL_BRINKMAN}
 
 # D3Q19, reference ordering (src/lbm/lattice_set.h:263-266)
 C = np.array([(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1),
@@ -35,7 +36,7 @@ class _Desc(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("model", ctypes.c_int), ("omega", ctypes.c_double),
                 ("cs_smag", ctypes.c_double), ("mrt_s", ctypes.c_double * 19),
-                ("op_lut", ctypes.c_uint8 * 256)]
+                ("op_lut", ctypes.c_uint8 * 256), ("alpha", ctypes.c_void_p)]
 
 
 _lib = None
@@ -123,6 +124,23 @@ class Lattice:
         self.tmp = np.empty_like(self.pops)
         self.rho = np.ones(self.N, dtype=self.dtype)
         self.u = np.zeros(3 * self.N, dtype=self.dtype)
+        self.alpha = None
+
+    def set_alpha(self, alpha):
+        """Per-cell Brinkman porosity for the brinkman model."""
+        self.alpha = np.ascontiguousarray(alpha, dtype=self.dtype).reshape(-1)
+        assert self.alpha.size == self.N
+        self.desc.alpha = self.alpha.ctypes.data
+
+    def objective_u2(self, key=2):
+        """J = sum over cells matching key of |u|^2, u = sum c f / (rho + alpha/2)."""
+        f = self.pops.reshape(19, self.N).astype(np.float64)
+        m = (self.flags & key) != 0
+        rho = f[:, m].sum(axis=0)
+        mom = C.T.astype(np.float64) @ f[:, m]
+        a = self.alpha[m].astype(np.float64) if self.alpha is not None else 0.0
+        u = mom / (rho + 0.5 * a)
+        return float((u * u).sum())
 
     def step(self, n=1):
         getattr(lib(), f"oracle_step_{self.suffix}")(ctypes.byref(self.desc), _ptr(self.flags),
@@ -136,13 +154,22 @@ class Lattice:
         return self.rho, self.u
 
 
-def cavity(ni, model="bgk", tau=0.53, ulid=0.1, cs=0.1, mrt_rate=1.2, dtype=np.float32):
+def cavity(ni, model="bgk", tau=0.53, ulid=0.1, cs=0.1, mrt_rate=1.2, dtype=np.float32,
+           alpha=None):
     """The reference lid-driven cavity (benchmarks/cavity3d/cavity3d.cpp:111-161)."""
     n = ni + 2
     flags = cavity_flags(ni)
     lat = Lattice(n, n, n, flags, model=model, tau=tau, cs=cs, mrt_rate=mrt_rate, dtype=dtype)
     lat.u.reshape(-1, 3)[flags == 8, 0] = lat.dtype.type(ulid)
+    if alpha is not None:
+        lat.set_alpha(alpha)
     return lat
+
+
+def porosity(ni, seed, amax=0.05):
+    """Seeded i.i.d. U[0, amax] porosity on the (ni+2)^3 stored mesh (float64)."""
+    n = ni + 2
+    return np.random.default_rng(seed).uniform(0.0, amax, size=n ** 3)
 
 
 # --------------------------------------------------------------------------- reference harness
@@ -165,7 +192,7 @@ def ref_binary(dtype=np.float32):
 
 
 def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float32,
-                  blockfile=None, threads=None, outdir=None):
+                  blockfile=None, threads=None, outdir=None, alpha=None):
     """Run the reference's own CPU path; returns (dict of arrays, mlups)."""
     exe = ref_binary(dtype)
     if exe is None:
@@ -177,6 +204,10 @@ def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float3
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
+    if alpha is not None:
+        afile = os.path.join(tempfile.mkdtemp(), "alpha.bin")
+        np.ascontiguousarray(alpha, dtype=dtype).tofile(afile)
+        env["FLB_ALPHA_FILE"] = afile
     args = [exe, model, str(ni), repr(float(tau)), repr(float(ulid)), str(steps), str(warmup),
             outdir, repr(float(cs))]
     if blockfile:

@@ -17,6 +17,10 @@
 //                   holds the local density of this step)
 //             mrt: collision::MRT_Feq_RhoU with the D3Q19 basis specialised in
 //                  mrt_d3q19_table.h (the reference ships only D2Q9 data)
+//             brinkman: BGK with a Brinkman drag F = -alpha u built from the
+//                  reference's own pieces (BrinkmanBGK below); per-cell alpha
+//                  read from the file named by FLB_ALPHA_FILE (N values of T,
+//                  reference cell order; zero when unset)
 //   Ni        interior cells per axis (stored mesh is (Ni+2)^3, one void layer)
 //   RT        relaxation time tau (lattice units; dx = dt = 1 so u_lid is lattice)
 //   blockfile optional BlockReader file (io/block_reader.h) for a multi-block run;
@@ -56,6 +60,39 @@ constexpr std::uint8_t VoidFlag = std::uint8_t(1);
 constexpr std::uint8_t AABBFlag = std::uint8_t(2);
 constexpr std::uint8_t BouncebackFlag = std::uint8_t(4);
 constexpr std::uint8_t BBMovingWallFlag = std::uint8_t(8);
+
+// Per-cell Brinkman porosity for the single-block run (FLB_ALPHA_FILE).
+static std::vector<T> g_alpha;
+
+// BGK with Brinkman drag F = -alpha u, assembled from the reference's own
+// components: the forced moment of moment::forcerhoUImpl (moment.h:408-422),
+// u = (sum c f + F/2) / rho, solved for F = -alpha u as u = sum c f / (rho + alpha/2);
+// force::ForcePop (force.h:29-36) for the discrete force; equilibrium::SecondOrder;
+// the update of collision::BGKForce (collision.h:61-90).
+template <typename CELL>
+struct BrinkmanBGK {
+  using LS = typename CELL::LatticeSet;
+  static void apply(CELL& cell) {
+    const T alpha = g_alpha.empty() ? T{} : g_alpha[cell.getId()];
+    T rho{};
+    Vector<T, LS::d> m{};
+    for (unsigned int i = 0; i < LS::q; ++i) {
+      rho += cell[i];
+      m += latset::c<LS>(i) * cell[i];
+    }
+    const Vector<T, LS::d> u = m / (rho + T{0.5} * alpha);
+    const Vector<T, LS::d> F = u * (-alpha);
+    std::array<T, LS::q> fi{};
+    force::ForcePop<T, LS>::compute(fi, u, F);
+    std::array<T, LS::q> feq{};
+    equilibrium::SecondOrder<CELL>::apply(feq, rho, u);
+    const T omega = cell.getOmega();
+    const T _omega = cell.get_Omega();
+    const T fomega = cell.getfOmega();
+    for (unsigned int i = 0; i < LS::q; ++i)
+      cell[i] = omega * feq[i] + _omega * cell[i] + fomega * fi[i];
+  }
+};
 
 struct Params {
   std::string model;
@@ -182,6 +219,20 @@ static void dispatch(const Params& p, GEO& Geo, BaseConverter<T>& BaseConv,
     ValuePack InitValues(BaseConv.getLatRhoInit(), Vector<T, 3>{}, T{});
     Runner<FIELDS, GEO>::template run<collision::MRT_Feq_RhoU<CELL>>(p, Geo, BaseConv,
                                                                       InitValues, cavity, toplid);
+  } else if (p.model == "brinkman") {
+    using FIELDS = TypePack<RHO<T>, VELOCITY<T, LatSet::d>, POP<T, LatSet::q>>;
+    using CELL = Cell<T, LatSet, FIELDS>;
+    ValuePack InitValues(BaseConv.getLatRhoInit(), Vector<T, 3>{}, T{});
+    if (const char* af = std::getenv("FLB_ALPHA_FILE")) {
+      std::ifstream in(af, std::ios::binary);
+      in.seekg(0, std::ios::end);
+      const std::size_t n = std::size_t(in.tellg()) / sizeof(T);
+      in.seekg(0);
+      g_alpha.resize(n);
+      in.read(reinterpret_cast<char*>(g_alpha.data()), n * sizeof(T));
+    }
+    Runner<FIELDS, GEO>::template run<BrinkmanBGK<CELL>>(p, Geo, BaseConv, InitValues, cavity,
+                                                         toplid);
   } else if (p.model == "les") {
     using FIELDS =
       TypePack<RHO<T>, VELOCITY<T, LatSet::d>, POP<T, LatSet::q>, SMAGORINSKY<T>>;

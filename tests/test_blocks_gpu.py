@@ -46,14 +46,14 @@ def test_blocks_match_reference_multiblock_golden(gpu_ok, name):
         assert np.array_equal(lat.download_flags(block=k), g[f"flags_b{k}"])
 
 
-@pytest.mark.parametrize("tile_y,ctas", [(8, 0), (2, 4), (1, 0)])
-def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas):
+@pytest.mark.parametrize("tile_y,ctas,vec", [(8, 0, 4), (2, 8, 2), (1, 0, 2), (4, 16, 4)])
+def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas, vec):
     """Uneven blocks with device halos reproduce the single-block run exactly on
     fluid cells, for every launch shape."""
     ni = 40
     blocks = G.uneven_blocks(ni, edges=(8, 12, 16), seed=5)
     lat = gpu_blocks(ni, blocks, "fp32")
-    lat.set_launch(tile_y, ctas)
+    lat.set_launch(tile_y, ctas, vec)
     lat.step(40)
     one = F.cavity(ni)
     one.step(40)
@@ -116,12 +116,14 @@ def test_graph_step_equals_plain_step(gpu_ok):
     assert np.array_equal(a.download_pops(), b.download_pops())
 
 
-def test_autotune_keeps_results_exact(gpu_ok):
-    a = F.cavity(36)
-    b = F.cavity(36)
-    ty, c, ms, taken = a.autotune(trial_steps=2)
-    assert ty in (1, 2, 4, 8) and c in (0, 2, 4, 8) and ms > 0 and taken > 0
-    assert a.get_launch() == (ty, c)
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp64"])
+def test_autotune_keeps_results_exact(gpu_ok, storage):
+    a = F.cavity(36, storage=storage)
+    b = F.cavity(36, storage=storage)
+    (ty, c, v), ms, taken = a.autotune(trial_steps=2)
+    assert ty in (1, 2, 4, 8) and c in (0, 8, 16, 32) and ms > 0 and taken > 0
+    assert v in ((1, 2) if storage == "fp64" else (2, 4))
+    assert a.get_launch() == (ty, c, v)
     b.step(taken)
     a.step(5)
     b.step(5)
@@ -134,3 +136,16 @@ def test_set_launch_rejects_bad_shapes(gpu_ok):
         a.set_launch(3, 0)
     with pytest.raises(F.FlbError):
         a.set_launch(8, -1)
+    with pytest.raises(F.FlbError):
+        a.set_launch(8, 0, 1)     # FP32 builds 2 or 4 cells per thread
+
+
+@pytest.mark.parametrize("storage,vec", [("fp32", 2), ("fp16s", 2), ("fp64", 1)])
+def test_every_vector_width_matches_oracle(gpu_ok, storage, vec):
+    lat = F.cavity(21, tau=0.55, storage=storage)
+    lat.set_launch(4, 0, vec)
+    lat.step(30)
+    ref = O.cavity(21, tau=0.55, dtype=np.float64 if storage == "fp64" else np.float32)
+    ref.step(30)
+    tol = {"fp32": 1e-5, "fp64": 1e-12, "fp16s": 2e-3}[storage]
+    assert rel_maxnorm(lat.download_pops(), ref.pops) < tol

@@ -146,3 +146,46 @@ def test_partition_axis_tiles_exactly():
     for seed in range(20):
         p = G.partition_axis(256, (32, 48, 64, 96), random.Random(seed))
         assert sum(p) == 256 and set(p) <= {32, 48, 64, 96}
+
+
+def test_brinkman_restatement_matches_reference_policy():
+    """The Brinkman-forced BGK restated in C against the reference-built policy
+    (reference ForcePop + SecondOrder + BGKForce update) in the harness."""
+    ni = 10
+    a = O.porosity(ni, 7)
+    for dt, tol in ((np.float64, 1e-13), (np.float32, 1e-5)):
+        if O.ref_binary(dt) is None:
+            pytest.skip("reference harness not built here")
+        ref = O.run_reference("brinkman", ni, 0.55, 0.1, 40, 0, dtype=dt, alpha=a, threads=2)
+        lat = O.cavity(ni, model="brinkman", tau=0.55, ulid=0.1, dtype=dt, alpha=a)
+        lat.step(40)
+        assert rel_maxnorm(lat.pops, ref["pops"]) < tol
+
+
+@pytest.mark.skipif(O.ref_binary(np.float64) is None, reason="reference harness not built here")
+def test_finite_difference_gradient_of_reference_solver():
+    """Central-difference dJ/dalpha of the reference CPU solver (Brinkman policy in
+    the harness) equals that of the restatement: the adjoint's FD oracle is pinned."""
+    ni, tau, steps, h = 6, 0.6, 25, 1e-4
+    a = O.porosity(ni, 2)
+    fl = O.cavity_flags(ni)
+    c = int(np.flatnonzero(fl == 2)[5])
+
+    def j_ref(al):
+        r = O.run_reference("brinkman", ni, tau, 0.1, steps, 0, dtype=np.float64, alpha=al,
+                            threads=1)
+        lat = O.cavity(ni, model="brinkman", tau=tau, dtype=np.float64, alpha=al)
+        lat.pops[:] = r["pops"]
+        return lat.objective_u2()
+
+    def j_orc(al):
+        lat = O.cavity(ni, model="brinkman", tau=tau, dtype=np.float64, alpha=al)
+        lat.step(steps)
+        return lat.objective_u2()
+
+    ap, am = a.copy(), a.copy()
+    ap[c] += h
+    am[c] -= h
+    g_ref = (j_ref(ap) - j_ref(am)) / (2 * h)
+    g_orc = (j_orc(ap) - j_orc(am)) / (2 * h)
+    assert abs(g_ref - g_orc) <= 1e-7 * abs(g_ref)
