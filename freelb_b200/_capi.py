@@ -99,6 +99,8 @@ SIGNATURES = {
                              ctypes.POINTER(ctypes.c_double), _P],
     "flb_adjoint_release": [_P],
     "flb_set_tasks": [_P, _I, _P, _P, _I],
+    "flb_reduce_conservation_noalloc": [_P, _P, ctypes.POINTER(Layout), _I, ctypes.c_double,
+                                        ctypes.c_uint8, ctypes.POINTER(ctypes.c_double), _P],
 }
 _RESTYPES = {"flb_last_error": ctypes.c_char_p}
 

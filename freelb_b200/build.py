@@ -17,8 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libflb_b200.so")
-SOURCES = ["flb_api.cu"]
-DEPS = ["flb_api.cu", "flb_kernels.cuh", "flb_lattice.cuh"]
+SOURCES = ["flb_api.cu", "flb_noalloc.cu"]
+DEPS = ["flb_api.cu", "flb_noalloc.cu", "flb_kernels.cuh", "flb_lattice.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -56,6 +56,15 @@ int fail(int code, const char* fmt, ...) {
 
 inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
+}  // namespace
+
+// Error reporting shared with the library's other translation units.
+namespace flb {
+int report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace flb
+
+namespace {
+
 struct HostBlock {
   LayoutParams L;   // this block's layout; L.dstride is the handle's direction stride
   long long base;   // element offset of the block inside every direction array

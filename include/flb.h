@@ -209,6 +209,35 @@ typedef struct flb_layout {
 FLB_API int flb_get_layout(const flb_lattice* lat, flb_layout* layout);
 FLB_API int flb_device_pointers(flb_lattice* lat, void** pops, void** flags, void** rho, void** vel);
 
+/* The same mass and momentum sums as flb_reduce_conservation, for callers that
+ * may not allocate GPU memory.  This entry point has no counterpart in the
+ * reference (FreeLB has no GPU reduction of this kind).
+ *
+ * Who needs it: a program whose GPU memory is handed out only by its own
+ * caching pool (so that memory accounting stays exact and no component
+ * triggers the implicit synchronisation a cudaMalloc/cudaFree can cause), or a
+ * latency-bound loop that must not wait on an allocation, cannot let this
+ * library call cudaMalloc behind its back.  Here the caller passes its own
+ * device pointers -- populations `pops` and `flags` laid out as `layout`
+ * describes (flb_get_layout / flb_device_pointers give both for a handle),
+ * `storage` (FLB_STORAGE_*) and `rho0` (the FP16S shift density) -- and a host
+ * array `out` for the four sums; the function allocates nothing.
+ *
+ * Its scratch is a fixed device array inside the library: 128 KiB, held on
+ * every GPU that loads the library until the process exits.  That bounds the
+ * lattice to 268,435,456 padded cells (layout->plane * layout->nz); larger
+ * layouts are rejected with FLB_ERR_INVALID.  The first call on a device looks
+ * up the array's device address for that device, so make that first call
+ * before capturing any stream.  Every call on a device uses the same scratch
+ * and it keeps the previous call's contents; nothing in it needs to start at
+ * zero (each call writes every slot it reads), but calls whose work overlaps
+ * on the GPU (different streams, different host threads) race on it and must
+ * be serialised by the caller.  `stream` orders the work and is synchronised
+ * before returning. */
+FLB_API int flb_reduce_conservation_noalloc(const void* pops, const uint8_t* flags,
+                                            const flb_layout* layout, int storage, double rho0,
+                                            uint8_t key, double out[4], void* stream);
+
 /* Per-block transfers of a multi-block handle (the functions above act on
  * block 0).  Replace BlockFieldManager::getBlockField(i) and
  * BlockLatticeManager::getBlockLat(i).getField<...>() access. */
