@@ -79,10 +79,18 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: begin the timed region only once
+        # it is sampling (at most 10 s)
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
@@ -162,6 +170,15 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------------------- our arm
+
+def max_over_ranks(torch, dist, value, device):
+    """Largest value over all ranks (the job time of independent replicas)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
 
 class DeviceTimer:
     """CUDA events on the launching stream, synchronised on both sides."""
@@ -281,22 +298,23 @@ def ensemble_block(F, torch, stream, steps, count=128, seed=0):
     return out
 
 
-def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=2, seed=0):
-    """C5: 128^3 cavity, Re = 500 (tau = 3*0.1*128/500 + 0.5), porosity alpha ~
+def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, seed=0):
+    """128^3 cavity, Re = 500 (tau = 3*0.1*128/500 + 0.5), porosity alpha ~
     U[0, 0.05]; J = sum |u|^2 at T = 2000; checkpoints every 100 steps; FP32
     forward and adjoint, FP64 gradient accumulation.  Reports the adjoint-to-
     forward time ratio and the gradient's relative error against FP64 central
-    differences (h = 1e-4) on a few seeded cells and on tau."""
+    differences (h = 1e-4) on 32 seeded fluid cells, on tau and on u_lid."""
     tau = 3 * 0.1 * ni / 500 + 0.5
     n = ni + 2
     alpha = np.random.default_rng(seed).uniform(0.0, 0.05, size=n ** 3)
 
-    def lattice(storage, a=alpha, t=tau):
-        lat = F.cavity(ni, tau=t, ulid=0.1, storage=storage, model="brinkman")
+    def lattice(storage, a=alpha, t=tau, ulid=0.1):
+        lat = F.cavity(ni, tau=t, ulid=ulid, storage=storage, model="brinkman")
         lat.upload_field("alpha", a.astype(lat.real))
         return lat
 
     lat = lattice("fp32")
+    lat.step(2, stream)
     with DeviceTimer(torch, stream) as tf:
         lat.step(steps, stream)
     lat.close()
@@ -307,8 +325,8 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=2, s
         g_alpha, g_tau, g_ulid = lat.adjoint_backward(stream=stream)
     lat.close()
 
-    def J(a=alpha, t=tau):
-        m = lattice("fp64", a, t)
+    def J(a=alpha, t=tau, ulid=0.1):
+        m = lattice("fp64", a, t, ulid)
         m.step(steps, stream)
         v = m.objective_u2(stream)
         m.close()
@@ -326,14 +344,19 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=2, s
         fd = (J(ap) - J(am)) / (2 * h)
         errs.append(abs(g_alpha[c] - fd) / abs(fd))
     fd_tau = (J(t=tau + h) - J(t=tau - h)) / (2 * h)
+    fd_ulid = (J(ulid=0.1 + h) - J(ulid=0.1 - h)) / (2 * h)
     return {"config": f"{ni}^3, T={steps}, checkpoints every {every}, tau={tau:.4f}",
             "forward_ms_per_step": tf.ms / steps,
             "forward_with_checkpoints_ms_per_step": tfc.ms / steps,
             "backward_ms_per_step": tb.ms / steps,
             "adjoint_to_forward_ratio": tb.ms / tf.ms,
             "dJ_dtau": g_tau, "dJ_dulid": g_ulid,
+            "fd_cells": int(fd_cells),
+            "fd_rel_err_alpha_max": float(np.max(errs)),
+            "fd_rel_err_alpha_median": float(np.median(errs)),
             "fd_rel_err_alpha": [float(e) for e in errs],
-            "fd_rel_err_tau": float(abs(g_tau - fd_tau) / abs(fd_tau))}
+            "fd_rel_err_tau": float(abs(g_tau - fd_tau) / abs(fd_tau)),
+            "fd_rel_err_ulid": float(abs(g_ulid - fd_ulid) / abs(fd_ulid))}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -353,13 +376,6 @@ def run_ours(args, rank, world, local_rank):
     cells = n ** 3
     stream = torch.cuda.current_stream(dev)
 
-    def max_over_ranks(ms):
-        if not dist:
-            return ms
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # headline: 512^3 BGK FP32, launch shape from the autotuner
     lat = F.cavity(ni, tau=0.53, ulid=0.1, storage=args.storage)
     if args.launch:
@@ -376,7 +392,7 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(local_rank) as cs:
         with DeviceTimer(torch, stream) as t:
             lat.step(args.steps, stream)
-    ms32 = max_over_ranks(t.ms)
+    ms32 = max_over_ranks(torch, dist, t.ms, dev)
     clocks = cs.summary()
     bad32 = lat.nonfinite()
     lat.close()
@@ -412,7 +428,7 @@ def run_ours(args, rank, world, local_rank):
         C.call("flb_download_field", lat._h, C.FIELD_VELOCITY,
                ctypes.c_void_p(out_u.ctypes.data), C.DTYPE_F32,
                ctypes.c_void_p(stream.cuda_stream))
-    e2e_ms = max_over_ranks(max(te.ms, (time.perf_counter() - t0) * 1000.0))
+    e2e_ms = max_over_ranks(torch, dist, max(te.ms, (time.perf_counter() - t0) * 1000.0), dev)
     lat.close()
     h2d = flags.nbytes + u0.nbytes
     d2h = out_rho.nbytes + out_u.nbytes

@@ -223,6 +223,32 @@ class Lattice:
         C.call("flb_check_finite", self._h, ctypes.byref(v), _stream(stream))
         return int(v.value)
 
+    def set_halo_mode(self, mode):
+        """"normal" (NormalCommunicate) or "full" (NormalFullCommunicate /
+        NormalAllCommunicate) halo exchange of a halo-mode block handle."""
+        C.call("flb_set_halo_mode", self._h, {"normal": C.HALO_NORMAL, "full": C.HALO_FULL}[mode])
+
+    # -- VTK output
+    def vtk_body(self, field, overlap=0, dtype=None, scale=None, offset=0.0, block=0,
+                 stream=None):
+        """Base64 body of the VTK DataArray of `field` ("rho", "u", "alpha" or
+        "flag") on `block` without `overlap` layers per side, converted to
+        `dtype` (float32 / float64; default: the lattice's arithmetic type) and,
+        with `scale`, mapped v -> v * scale + offset in that type first: the
+        characters the reference's vtmo writers put between the DataArray tags."""
+        fid = C.VTK_FLAG if field == "flag" else FIELDS[field]
+        dt = np.dtype(dtype or self.real)
+        odt = C.DTYPE_F64 if dt == np.float64 else C.DTYPE_F32
+        mp = 0 if scale is None else 1
+        sc = 1.0 if scale is None else float(scale)
+        n = ctypes.c_size_t()
+        C.call("flb_vtk_field_base64", self._h, int(block), fid, int(overlap), odt, mp, sc,
+               float(offset), None, 0, ctypes.byref(n), _stream(stream))
+        buf = ctypes.create_string_buffer(n.value)
+        C.call("flb_vtk_field_base64", self._h, int(block), fid, int(overlap), odt, mp, sc,
+               float(offset), buf, n.value, ctypes.byref(n), _stream(stream))
+        return buf.raw[:n.value].decode()
+
     # -- objective and discrete adjoint
     def objective_u2(self, stream=None):
         """J = sum over bulk cells of |u|^2 (forced moment with the alpha field)."""
@@ -258,6 +284,48 @@ class Lattice:
         v = ctypes.c_size_t()
         C.call("flb_memory_bytes", self._h, ctypes.byref(v))
         return int(v.value)
+
+
+BB_KINDS = {"normal": C.BB_NORMAL, "movingwall": C.BB_MOVINGWALL,
+            "anti_simple": C.BB_ANTI_SIMPLE, "anti_o1": C.BB_ANTI_O1, "anti_o2": C.BB_ANTI_O2,
+            "anti_pressure": C.BB_ANTI_PRESSURE}
+
+
+class BounceBackManager:
+    """Post-stream halfway bounce-back on a single-block lattice:
+    BBLikeFixedBlockBdManager<bounceback::KIND<CELL>, ...> with KIND one of
+    normal, movingwall, anti_simple, anti_O1, anti_O2, anti_pressure
+    (src/boundary/bounce_back_boundary.h:167-256).  apply() after each step, as
+    BlockBoundaryManager::Apply() after Stream()."""
+
+    def __init__(self, lattice, cell_flag, void_flag=1, kind="normal", rho0=1.0):
+        if kind not in BB_KINDS:
+            raise ValueError(f"unknown bounce-back kind {kind!r}; one of {sorted(BB_KINDS)}")
+        self.lattice = lattice
+        self.kind = kind
+        h = ctypes.c_void_p()
+        C.call("flb_bb_create", lattice._h, int(cell_flag), int(void_flag), BB_KINDS[kind],
+               float(rho0), ctypes.byref(h))
+        self._h = h
+
+    def counts(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        C.call("flb_bb_count", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def apply(self, stream=None):
+        C.call("flb_bb_apply", self._h, self.lattice._h, _stream(stream))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            C.load().flb_bb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def cavity_flags(ni: int) -> np.ndarray:

@@ -101,7 +101,18 @@ SIGNATURES = {
     "flb_set_tasks": [_P, _I, _P, _P, _I],
     "flb_reduce_conservation_noalloc": [_P, _P, ctypes.POINTER(Layout), _I, ctypes.c_double,
                                         ctypes.c_uint8, ctypes.POINTER(ctypes.c_double), _P],
+    "flb_bb_create": [_P, ctypes.c_uint8, ctypes.c_uint8, _I, ctypes.c_double,
+                      ctypes.POINTER(_P)],
+    "flb_bb_count": [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+    "flb_bb_apply": [_P, _P, _P],
+    "flb_bb_destroy": [_P],
+    "flb_set_halo_mode": [_P, _I],
+    "flb_vtk_field_base64": [_P, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _P],
 }
+VTK_FLAG = 16
+HALO_NORMAL, HALO_FULL = 0, 1
+BB_NORMAL, BB_MOVINGWALL, BB_ANTI_SIMPLE, BB_ANTI_O1, BB_ANTI_O2, BB_ANTI_PRESSURE = range(6)
 _RESTYPES = {"flb_last_error": ctypes.c_char_p}
 
 _lib = None

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libflb_b200.so")
-SOURCES = ["flb_api.cu", "flb_noalloc.cu"]
+SOURCES = ["flb_api.cu", "flb_noalloc.cu", "flb_boundary.cu"]
 DEPS = ["flb_api.cu", "flb_noalloc.cu", "flb_kernels.cuh", "flb_lattice.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -61,17 +61,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+EXAMPLES = ("cavity3d_b200", "cavity3d_vtk")
 EXAMPLE_SRC = os.path.join(HERE, "cpp", "examples", "cavity3d_b200.cpp")
 EXAMPLE_BIN = os.path.join(HERE, "cpp", "_build", "cavity3d_b200")
 
 
-def build_examples(force: bool = False) -> str:
-    """Compile the C++17 host-class example against libflb_b200.so (g++)."""
-    deps = [EXAMPLE_SRC, os.path.join(HERE, "cpp", "freelb.h"), LIB]
-    if not force and not _stale(EXAMPLE_BIN, deps):
-        return EXAMPLE_BIN
-    os.makedirs(os.path.dirname(EXAMPLE_BIN), exist_ok=True)
-    cmd = ["g++", "-std=c++17", "-O2", "-o", EXAMPLE_BIN, EXAMPLE_SRC, "-L" + HERE, "-lflb_b200",
+def build_example(name: str, force: bool = False) -> str:
+    """Compile one C++17 host-class example against libflb_b200.so (g++)."""
+    src = os.path.join(HERE, "cpp", "examples", name + ".cpp")
+    out = os.path.join(HERE, "cpp", "_build", name)
+    deps = [src, os.path.join(HERE, "cpp", "freelb.h"), LIB]
+    if not force and not _stale(out, deps):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-o", out, src, "-L" + HERE, "-lflb_b200",
            "-Wl,-rpath,$ORIGIN/../.."]
     env = dict(os.environ)
     env.pop("CC", None)
@@ -79,6 +82,13 @@ def build_examples(force: bool = False) -> str:
     res = subprocess.run(cmd, capture_output=True, text=True, env=env)
     if res.returncode != 0:
         raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    return out
+
+
+def build_examples(force: bool = False) -> str:
+    """Compile every example; returns the cavity example's path."""
+    for name in EXAMPLES:
+        build_example(name, force)
     return EXAMPLE_BIN
 
 

@@ -1,12 +1,15 @@
 // cavity3d_b200.cpp -- the lid-driven cavity through the C++17 host classes.
 //
-//   cavity3d_b200 <Ni> <tau> <u_lid> <steps> [model: bgk|mrt|les] [out.bin]
+//   cavity3d_b200 <Ni> <tau> <u_lid> <steps> [model: bgk|mrt|les|halfway] [out.bin]
 //
 // Written against the reference's programming interface (geometry, flag
 // field, converter, task selector, BlockLatticeManager): the same calls a
 // FreeLB cavity program makes, executed on the GPU.  With an output path it
 // writes rho (N values) then u (3N values) as float64 after refreshing them on
-// the fluid cells with the moment::rhoU<CELL,true> task.
+// the fluid cells with the moment::rhoU<CELL,true> task.  Model "halfway"
+// collides wall and lid cells like fluid (BGK) and applies the post-stream
+// halfway bounce-back managers after every Stream(), as
+// examples/couette2d/couette2d.cpp does.
 #include <cstdlib>
 #include <string>
 
@@ -14,7 +17,7 @@
 
 int Thread_Num = 1;
 
-template <typename Bulk, typename CELL, typename FIELDS>
+template <typename Bulk, typename CELL, typename FIELDS, bool Halfway = false>
 int run(int Ni, double tau, double ulid, int steps, const char* out) {
   using T = float;
   using LatSet = D3Q19<T>;
@@ -38,12 +41,30 @@ int run(int Ni, double tau, double ulid, int steps, const char* out) {
   using NSTask = TaskSelector<std::uint8_t, CELL, tmp::Key_TypePair<AABBFlag, Bulk>,
                               tmp::Key_TypePair<BouncebackFlag, collision::BounceBack<CELL>>,
                               tmp::Key_TypePair<BBMovingWallFlag, collision::BounceBackMovingWall<CELL>>>;
+  using HWTask = TaskSelector<std::uint8_t, CELL,
+                              tmp::Key_TypePair<AABBFlag | BouncebackFlag | BBMovingWallFlag, Bulk>>;
   using RhoU = TaskSelector<std::uint8_t, CELL, tmp::Key_TypePair<AABBFlag, moment::rhoU<CELL, true>>>;
+  using LM = BlockLatticeManager<T, LatSet, FIELDS>;
+  using FM = BlockFieldManager<FLAG, T, 3>;
   Timer timer;
-  while (timer() < steps) {
-    NS.template ApplyCellDynamics<NSTask>(FlagFM);
-    NS.Stream();
-    ++timer;
+  if constexpr (Halfway) {
+    BBLikeFixedBlockBdManager<bounceback::normal<CELL>, LM, FM> NS_BB("NS_BB", NS, FlagFM,
+                                                                      BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::movingwall<CELL>, LM, FM> NS_BBMW(
+        "NS_BBMW", NS, FlagFM, BBMovingWallFlag, VoidFlag);
+    BlockBoundaryManager BM(&NS_BB, &NS_BBMW);
+    while (timer() < steps) {
+      NS.template ApplyCellDynamics<HWTask>(FlagFM);
+      NS.Stream();
+      BM.Apply();
+      ++timer;
+    }
+  } else {
+    while (timer() < steps) {
+      NS.template ApplyCellDynamics<NSTask>(FlagFM);
+      NS.Stream();
+      ++timer;
+    }
   }
   timer.Print_MainLoopPerformance(Geo.getTotalCellNum());
   NS.template ApplyCellDynamics<RhoU>(FlagFM);
@@ -79,6 +100,9 @@ int main(int argc, char** argv) {
   using CELL = Cell<T, D3Q19<T>, FIELDS>;
   try {
     if (model == "mrt") return run<collision::MRT_Feq_RhoU<CELL>, CELL, FIELDS>(Ni, tau, ulid, steps, out);
+    if (model == "halfway")
+      return run<collision::BGK<moment::rhoU<CELL>, equilibrium::SecondOrder<CELL>>, CELL, FIELDS,
+                 true>(Ni, tau, ulid, steps, out);
     if (model == "les")
       return run<collision::SmagorinskyBGK<moment::rhoU<CELL, true>, equilibrium::SecondOrder<CELL>>,
                  CELL, FIELDS>(Ni, tau, ulid, steps, out);

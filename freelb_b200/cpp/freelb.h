@@ -25,12 +25,16 @@
 // (multi-block equivalence is tested on the C ABI).
 #pragma once
 
+#include <sys/stat.h>
+
 #include <array>
+#include <functional>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
 #include <limits>
 #include <map>
@@ -42,6 +46,8 @@
 #include <vector>
 
 #include "../../include/flb.h"
+#include "../../include/flb_boundary.h"
+#include "../../include/flb_vtk.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -318,13 +324,14 @@ class BlockGeometry3D {
   int blocknum_;
   T voxel_;
   Vector<T, 3> min_ext_;
+  int overlap_;
 
  public:
   BlockGeometry3D(int Nx, int Ny, int Nz, int blocknum, const AABB<T, 3>& block, T voxelSize,
                   int overlap = 1)
       : nx_(Nx + 2 * overlap), ny_(Ny + 2 * overlap), nz_(Nz + 2 * overlap),
         blocknum_(blocknum), voxel_(voxelSize),
-        min_ext_(block.getMin() - Vector<T, 3>(voxelSize * T(overlap))) {
+        min_ext_(block.getMin() - Vector<T, 3>(voxelSize * T(overlap))), overlap_(overlap) {
     std::cout << "[BlockGeometry3D]:\n  Total CellNum: " << getTotalCellNum()
               << "\n  BlockNum: 1 (device block; requested " << blocknum << ")" << std::endl;
   }
@@ -335,6 +342,10 @@ class BlockGeometry3D {
   std::size_t getN() const { return getTotalCellNum(); }
   int getBlockNum() const { return 1; }
   T getVoxelSize() const { return voxel_; }
+  int getOverlap() const { return overlap_; }
+  Vector<int, 3> getMesh() const { return Vector<int, 3>(nx_, ny_, nz_); }
+  // centre of the first stored cell (basic_geometry.hh:298: _min + VoxelSize / 2)
+  Vector<T, 3> getMinCenter() const { return min_ext_ + Vector<T, 3>(T(0.5) * voxel_); }
   // MinCenter + VoxelSize * (i, j, k) (basic_geometry.h:245, 310-311)
   Vector<T, 3> getVoxel(int i, int j, int k) const {
     const T h = T(0.5) * voxel_;
@@ -461,6 +472,15 @@ class BlockFieldManager {
   const field_t& field() const { return field_; }
   const BlockGeometry3D<T>& geo() const { return geo_; }
   void copyToDevice() { field_.dirty = true; }
+  // For the RHO and VELOCITY managers of a BlockLatticeManager: the device
+  // copy the VTK writers encode from, and the call that uploads host edits
+  // to it first.
+  struct DeviceView {
+    flb_lattice* lat = nullptr;
+    int field = -1;
+    std::function<void()> sync;
+  };
+  DeviceView device;
 
  private:
   const BlockGeometry3D<T>& geo_;
@@ -607,9 +627,12 @@ class BlockLatticeManager {
     d.omega = double(conv.getOMEGA());
     d.storage = std::is_same<T, double>::value ? FLB_STORAGE_FP64 : FLB_STORAGE_FP32;
     d.rho0 = double(conv.getLatRhoInit());
+    rho0_ = d.rho0;
     d.ntasks = 0;
     init_smagorinsky(d, init);
     flbcpp::check(flb_create(&d, &h_), "flb_create");
+    vel_.device = {h_, FLB_FIELD_VELOCITY, [this] { push_fields(); }};
+    rho_.device = {h_, FLB_FIELD_RHO, [this] { push_fields(); }};
   }
   ~BlockLatticeManager() { flb_destroy(h_); }
   BlockLatticeManager(const BlockLatticeManager&) = delete;
@@ -669,6 +692,11 @@ class BlockLatticeManager {
     return T(v);
   }
   flb_lattice* handle() { return h_; }
+  // Bring the device copies of the flags and fields up to date (what the
+  // next ApplyCellDynamics would do); used by the boundary managers.
+  template <typename FlagManager>
+  void sync(FlagManager& flags) { push(flags); }
+  double rho0() const { return rho0_; }
 
  private:
   template <typename INIT>
@@ -683,6 +711,9 @@ class BlockLatticeManager {
       flbcpp::check(flb_upload_flags(h_, f.data.data(), nullptr), "flb_upload_flags");
       f.dirty = false;
     }
+    push_fields();
+  }
+  void push_fields() {
     if (vel_.field().dirty) {
       std::vector<T> buf(3 * vel_.field().data.size());
       for (std::size_t i = 0; i < vel_.field().data.size(); ++i)
@@ -718,42 +749,452 @@ class BlockLatticeManager {
   VelField vel_;
   RhoField rho_;
   flb_lattice* h_ = nullptr;
+  double rho0_ = 1.0;
   bool pending_ = false;
   bool fields_stale_ = false;
   bool tolerance_on_ = false;
 };
 
 // ---------------------------------------------------------------------------
-// post-stream boundary managers (src/boundary/boundary.h:34-222) are the
-// halfway bounce-back of the reference; the cavity programs construct them but
-// run their wall physics through the BounceBack / BounceBackMovingWall tasks.
+// post-stream boundary managers (src/boundary/boundary.h:34-222): halfway
+// bounce-back after Stream() on the device (flb_boundary.h).  The policy tags
+// carry the device kind of bounce_back_boundary.h:167-256.
 namespace bounceback {
 template <typename CELL>
-struct normal {};
+struct normal { static constexpr int kind = FLB_BB_NORMAL; };
 template <typename CELL>
-struct movingwall {};
+struct movingwall { static constexpr int kind = FLB_BB_MOVINGWALL; };
+template <typename CELL>
+struct anti_simple { static constexpr int kind = FLB_BB_ANTI_SIMPLE; };
+template <typename CELL>
+struct anti_O1 { static constexpr int kind = FLB_BB_ANTI_O1; };
+template <typename CELL>
+struct anti_O2 { static constexpr int kind = FLB_BB_ANTI_O2; };
+template <typename CELL>
+struct anti_pressure { static constexpr int kind = FLB_BB_ANTI_PRESSURE; };
 }  // namespace bounceback
 
-template <typename BBType, typename LatticeManager, typename FlagManager>
-class BBLikeFixedBlockBdManager {
+class AbstractBlockBoundary {
  public:
-  BBLikeFixedBlockBdManager(std::string name, LatticeManager&, FlagManager&, std::uint8_t,
-                            std::uint8_t)
-      : name_(std::move(name)) {}
-  void Apply() {
-    throw std::logic_error(name_ + ": post-stream bounce-back managers are not built on the "
-                                   "device; use the BounceBack / BounceBackMovingWall tasks");
+  virtual ~AbstractBlockBoundary() = default;
+  virtual void Apply() = 0;
+  virtual void Apply(std::int64_t) { Apply(); }
+};
+
+// BBLikeFixedBlockBdManager (boundary.h:86-140): the boundary cells and their
+// outflow directions are found from the flags at construction, like
+// BlockFixedBoundary::Setup; Apply() runs after Stream().
+template <typename BBType, typename LatticeManager, typename FlagManager>
+class BBLikeFixedBlockBdManager final : public AbstractBlockBoundary {
+ public:
+  BBLikeFixedBlockBdManager(std::string name, LatticeManager& lat, FlagManager& flags,
+                            std::uint8_t cellflag, std::uint8_t voidflag = std::uint8_t(1))
+      : name_(std::move(name)), lat_(lat) {
+    lat.sync(flags);
+    flbcpp::check(flb_bb_create(lat.handle(), cellflag, voidflag, BBType::kind, lat.rho0(), &h_),
+                  "flb_bb_create");
+  }
+  ~BBLikeFixedBlockBdManager() override { flb_bb_destroy(h_); }
+  BBLikeFixedBlockBdManager(const BBLikeFixedBlockBdManager&) = delete;
+  BBLikeFixedBlockBdManager& operator=(const BBLikeFixedBlockBdManager&) = delete;
+
+  void Apply() override {
+    flbcpp::check(flb_bb_apply(h_, lat_.handle(), nullptr), "flb_bb_apply");
+  }
+  void Apply(std::int64_t) override { Apply(); }  // one refinement level
+  void getinfo() const {
+    long long cells = 0;
+    flb_bb_count(h_, &cells, nullptr);
+    std::cout << std::setw(18) << std::left << name_ << std::setw(10) << std::left << cells
+              << std::endl;
   }
 
  private:
   std::string name_;
+  LatticeManager& lat_;
+  flb_bb* h_ = nullptr;
 };
 
+// BlockBoundaryManager (basic_boundary.h:331-348): applies its managers in order.
 class BlockBoundaryManager {
  public:
+  explicit BlockBoundaryManager(std::vector<AbstractBlockBoundary*> bds) : bds_(std::move(bds)) {}
   template <typename... B>
-  explicit BlockBoundaryManager(B*...) {}
+  explicit BlockBoundaryManager(B*... bs) : bds_{static_cast<AbstractBlockBoundary*>(bs)...} {}
   void Apply() {
-    throw std::logic_error("post-stream bounce-back managers are not built on the device");
+    for (AbstractBlockBoundary* b : bds_) b->Apply();
   }
+  void Apply(std::int64_t count) {
+    for (AbstractBlockBoundary* b : bds_) b->Apply(count);
+  }
+
+ private:
+  std::vector<AbstractBlockBoundary*> bds_;
 };
+
+// ---------------------------------------------------------------------------
+// VTK output (src/io/vtm_writer.h:288-663, namespace vtmo; src/io/vti_writer.h:
+// 424-986, namespace vtino): one .vti per block plus a .vtm index under
+// ./vtkoutput/vtidata/, written byte for byte as the reference writes them.
+// Fields resident on the device (the lattice's RHO and VELOCITY) are cropped,
+// converted and base64-encoded on the GPU (flb_vtk_field_base64); host fields
+// (the flag field) are encoded here.
+namespace flbcpp {
+inline void mkdir_one(const std::string& d) { ::mkdir(d.c_str(), 0755); }
+template <typename X>
+struct ident {  // keeps a parameter out of class template argument deduction
+  using type = X;
+};
+inline void make_dir(const std::string& d) {
+  std::string cur;
+  for (char c : d) {
+    cur += c;
+    if (c == '/') mkdir_one(cur);
+  }
+  mkdir_one(cur);
+}
+// RFC 4648 base64 with '=' padding, one stream (src/io/base64.h Base64Encoder)
+inline void base64_append(std::string& out, const unsigned char* p, std::size_t n) {
+  static const char* a = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
+  std::size_t i = 0;
+  for (; i + 3 <= n; i += 3) {
+    out += a[p[i] >> 2];
+    out += a[((p[i] & 3) << 4) | (p[i + 1] >> 4)];
+    out += a[((p[i + 1] & 15) << 2) | (p[i + 2] >> 6)];
+    out += a[p[i + 2] & 63];
+  }
+  if (i < n) {
+    const unsigned b0 = p[i], b1 = i + 1 < n ? p[i + 1] : 0u;
+    out += a[b0 >> 2];
+    out += a[((b0 & 3) << 4) | (b1 >> 4)];
+    out += i + 1 < n ? a[(b1 & 15) << 2] : '=';
+    out += '=';
+  }
+}
+// DataArray body of host values: size block, then the data
+template <typename V>
+std::string base64_body(const std::vector<V>& v) {
+  std::string s;
+  const unsigned size = unsigned(v.size() * sizeof(V));
+  base64_append(s, reinterpret_cast<const unsigned char*>(&size), sizeof size);
+  base64_append(s, reinterpret_cast<const unsigned char*>(v.data()), v.size() * sizeof(V));
+  return s;
+}
+template <typename V>
+std::string device_body(flb_lattice* lat, int field, int overlap, int map, double scale,
+                        double offset) {
+  const int dt = std::is_same<V, double>::value ? FLB_DTYPE_F64 : FLB_DTYPE_F32;
+  std::size_t len = 0;
+  check(flb_vtk_field_base64(lat, 0, field, overlap, dt, map, scale, offset, nullptr, 0, &len,
+                             nullptr),
+        "flb_vtk_field_base64");
+  std::string s(len, '\0');
+  check(flb_vtk_field_base64(lat, 0, field, overlap, dt, map, scale, offset, &s[0], len, &len,
+                             nullptr),
+        "flb_vtk_field_base64");
+  return s;
+}
+template <typename V>
+const char* vtk_type() {
+  if constexpr (std::is_same<V, double>::value) return "Float64";
+  else if constexpr (std::is_same<V, float>::value) return "Float32";
+  else if constexpr (std::is_same<V, std::uint8_t>::value) return "UInt8";
+  else if constexpr (std::is_same<V, std::int8_t>::value) return "Int8";
+  else if constexpr (std::is_same<V, std::int32_t>::value) return "Int32";
+  else static_assert(sizeof(V) == 0, "no VTK type for this value type");
+}
+// cells [ov, n - ov) of a host array, x fastest (util::CopyFromFieldArray)
+template <typename V, typename F>
+std::vector<V> crop(const Vector<int, 3>& mesh, int ov, std::size_t n, F&& at) {
+  std::vector<V> out;
+  out.reserve(n);
+  for (int k = ov; k < mesh[2] - ov; ++k)
+    for (int j = ov; j < mesh[1] - ov; ++j)
+      for (int i = ov; i < mesh[0] - ov; ++i)
+        at(out, std::size_t(i) + std::size_t(mesh[0]) * (std::size_t(j) + std::size_t(mesh[1]) * k));
+  return out;
+}
+// f(x) == x * scale + offset (offset 0: x * scale) for probe values, bit for bit
+template <typename V>
+bool affine(const std::function<V(V)>& f, double& scale, double& offset) {
+  const V o = f(V(0)), sc = f(V(1)) - o;
+  for (V x : {V(0.5), V(2), V(-3), V(1.25e-3), V(7.75)}) {
+    const V want = o == V(0) ? x * sc : x * sc + o;
+    if (!(f(x) == want)) return false;
+  }
+  scale = double(sc);
+  offset = double(o);
+  return true;
+}
+}  // namespace flbcpp
+
+namespace vtmo {
+class AbstractWriter {
+ public:
+  virtual ~AbstractWriter() = default;
+  virtual void writeBinary(const std::string& fName, int Overlap) const = 0;
+};
+class AbstWriterSet {
+ public:
+  virtual ~AbstWriterSet() = default;
+  virtual const AbstractWriter& getWriter(int i) const = 0;
+};
+
+namespace detail {
+inline void open_array(const std::string& fName, const char* type, const std::string& name,
+                       unsigned ncomp) {
+  std::ofstream f(fName, std::ios::out | std::ios::app);
+  f << "<DataArray type=\"" << type << "\" Name=\"" << name << "\" "
+    << "format=\"binary\" encoding=\"base64\" " << "NumberOfComponents=\"" << ncomp
+    << "\">\n";
+}
+inline void body_and_close(const std::string& fName, const std::string& body) {
+  {
+    std::ofstream fb(fName, std::ios::out | std::ios::app | std::ios::binary);
+    fb.write(body.data(), std::streamsize(body.size()));
+  }
+  std::ofstream ff(fName, std::ios::out | std::ios::app);
+  ff << "\n</DataArray>\n";
+}
+}  // namespace detail
+
+// Scalar field of one block; Phys form maps values through `f` first.
+template <typename Manager, typename V>
+class ScalarArrayWriter final : public AbstractWriter {
+ public:
+  ScalarArrayWriter(std::string name, const Manager& fm, std::function<V(V)> f)
+      : name_(std::move(name)), fm_(fm), f_(std::move(f)) {}
+  void writeBinary(const std::string& fName, int Overlap) const override {
+    detail::open_array(fName, flbcpp::vtk_type<V>(), name_, 1);
+    detail::body_and_close(fName, body(Overlap));
+  }
+
+ private:
+  std::string body(int ov) const {
+    double scale = 1, offset = 0;
+    const bool phys = bool(f_);
+    if (fm_.device.lat && (!phys || flbcpp::affine<V>(f_, scale, offset))) {
+      fm_.device.sync();
+      return flbcpp::device_body<V>(fm_.device.lat, fm_.device.field, ov, phys ? 1 : 0, scale,
+                                    offset);
+    }
+    const auto& d = fm_.field().data;
+    const Vector<int, 3> mesh = fm_.geo().getMesh();
+    return flbcpp::base64_body(flbcpp::crop<V>(mesh, ov, d.size(), [&](std::vector<V>& o, std::size_t id) {
+      o.push_back(phys ? f_(V(d[id])) : V(d[id]));
+    }));
+  }
+  std::string name_;
+  const Manager& fm_;
+  std::function<V(V)> f_;
+};
+
+template <typename Manager, typename V>
+class VectorArrayWriter final : public AbstractWriter {
+ public:
+  using Vec = Vector<V, 3>;
+  VectorArrayWriter(std::string name, const Manager& fm, std::function<Vec(Vec)> f)
+      : name_(std::move(name)), fm_(fm), f_(std::move(f)) {}
+  void writeBinary(const std::string& fName, int Overlap) const override {
+    detail::open_array(fName, flbcpp::vtk_type<V>(), name_, 3);
+    detail::body_and_close(fName, body(Overlap));
+  }
+
+ private:
+  std::string body(int ov) const {
+    double scale = 1, offset = 0;
+    const bool phys = bool(f_);
+    bool dev = fm_.device.lat != nullptr;
+    if (dev && phys) {
+      // component-wise affine map with the same factor on every component
+      const std::function<V(V)> g = [this](V x) { return f_(Vec(x))[0]; };
+      dev = flbcpp::affine<V>(g, scale, offset);
+      for (V x : {V(0.5), V(-2)})
+        for (int c = 0; c < 3; ++c) {
+          Vec in(V(0));
+          in[c] = x;
+          const Vec out = f_(in);
+          for (int e = 0; e < 3; ++e)
+            if (!(out[e] == (e == c ? g(x) : g(V(0))))) dev = false;
+        }
+    }
+    if (dev) {
+      fm_.device.sync();
+      return flbcpp::device_body<V>(fm_.device.lat, fm_.device.field, ov, phys ? 1 : 0, scale,
+                                    offset);
+    }
+    const auto& d = fm_.field().data;
+    const Vector<int, 3> mesh = fm_.geo().getMesh();
+    return flbcpp::base64_body(
+        flbcpp::crop<V>(mesh, ov, 3 * d.size(), [&](std::vector<V>& o, std::size_t id) {
+          const Vec v = phys ? f_(d[id]) : d[id];
+          for (int c = 0; c < 3; ++c) o.push_back(V(v[c]));
+        }));
+  }
+  std::string name_;
+  const Manager& fm_;
+  std::function<Vec(Vec)> f_;
+};
+
+// vtmo::ScalarWriter / PhysScalarWriter / VectorWriter / PhysVectorWriter:
+// one array writer per block (one device block here).
+template <typename FieldType, typename FloatType, unsigned int Dim>
+class ScalarWriter final : public AbstWriterSet {
+  using Manager = BlockFieldManager<FieldType, FloatType, Dim>;
+
+ public:
+  ScalarWriter(std::string varname, const BlockFieldManager<FieldType, FloatType, Dim>& fm)
+      : w_(std::move(varname), fm, nullptr) {}
+  const AbstractWriter& getWriter(int) const override { return w_; }
+
+ private:
+  ScalarArrayWriter<Manager, typename FieldType::value_type> w_;
+};
+template <typename FieldType, typename FloatType, unsigned int Dim>
+class PhysScalarWriter final : public AbstWriterSet {
+  using Manager = BlockFieldManager<FieldType, FloatType, Dim>;
+  using V = typename FieldType::value_type;
+
+ public:
+  PhysScalarWriter(std::string varname, const BlockFieldManager<FieldType, FloatType, Dim>& fm,
+                   typename flbcpp::ident<std::function<V(V)>>::type f)
+      : w_(std::move(varname), fm, std::move(f)) {}
+  const AbstractWriter& getWriter(int) const override { return w_; }
+
+ private:
+  ScalarArrayWriter<Manager, V> w_;
+};
+template <typename FieldType, typename FloatType, unsigned int Dim>
+class VectorWriter final : public AbstWriterSet {
+  using Manager = BlockFieldManager<FieldType, FloatType, Dim>;
+
+ public:
+  VectorWriter(std::string varname, const BlockFieldManager<FieldType, FloatType, Dim>& fm)
+      : w_(std::move(varname), fm, nullptr) {}
+  const AbstractWriter& getWriter(int) const override { return w_; }
+
+ private:
+  VectorArrayWriter<Manager, FloatType> w_;
+};
+template <typename FieldType, typename FloatType, unsigned int Dim>
+class PhysVectorWriter final : public AbstWriterSet {
+  using Manager = BlockFieldManager<FieldType, FloatType, Dim>;
+  using Vec = Vector<FloatType, 3>;
+
+ public:
+  PhysVectorWriter(std::string varname, const BlockFieldManager<FieldType, FloatType, Dim>& fm,
+                   typename flbcpp::ident<std::function<Vec(Vec)>>::type f)
+      : w_(std::move(varname), fm, std::move(f)) {}
+  const AbstractWriter& getWriter(int) const override { return w_; }
+
+ private:
+  VectorArrayWriter<Manager, FloatType> w_;
+};
+
+// vtino::vtiManager with overlap (vti_writer.h:438-548)
+template <typename T, unsigned int Dim>
+class vtiManager {
+ public:
+  vtiManager(std::string filename, int id, T voxsize, Vector<T, Dim> min, Vector<int, Dim> ext,
+             int Overlap)
+      : filename_(std::move(filename)), id_(id), voxel_(voxsize), overlap_(Overlap),
+        min_(min + Vector<T, Dim>(T(Overlap) * voxsize)),
+        ext_(ext - Vector<int, Dim>(2 * Overlap)) {
+    flbcpp::make_dir(dirname_);
+  }
+  void addWriter(const AbstractWriter& w) { writers_.push_back(&w); }
+  void WriteBinary() { write(dirname_ + filename_ + "_B" + std::to_string(id_) + ".vti"); }
+  void WriteBinary(int step) {
+    write(dirname_ + filename_ + "_T" + std::to_string(step) + "_B" + std::to_string(id_) +
+          ".vti");
+  }
+
+ private:
+  void write(const std::string& fullName) {
+    {
+      std::ofstream f(fullName);
+      f << "<?xml version=\"1.0\"?>\n";
+      f << "<VTKFile type=\"ImageData\" version=\"0.1\" " << "byte_order=\"LittleEndian\">\n";
+      f << "<ImageData WholeExtent=\"" << 0 << " " << ext_[0] << " " << 0 << " " << ext_[1] << " "
+        << 0 << " " << ext_[2] << "\" Origin=\"" << min_[0] << " " << min_[1] << " " << min_[2]
+        << "\" Spacing=\"" << voxel_ << " " << voxel_ << " " << voxel_ << "\">\n";
+      f << "<Piece Extent=\"" << 0 << " " << ext_[0] << " " << 0 << " " << ext_[1] << " " << 0
+        << " " << ext_[2] << "\">\n";
+      f << "<PointData>\n";
+    }
+    for (const AbstractWriter* w : writers_) w->writeBinary(fullName, overlap_);
+    std::ofstream f(fullName, std::ios::app);
+    f << "</PointData>\n";
+    f << "</Piece>\n";
+    f << "</ImageData>\n";
+    f << "</VTKFile>\n";
+  }
+  std::string dirname_ = "./vtkoutput/vtidata/";
+  std::string filename_;
+  int id_;
+  T voxel_;
+  int overlap_;
+  Vector<T, Dim> min_;
+  Vector<int, Dim> ext_;
+  std::vector<const AbstractWriter*> writers_;
+};
+
+// vtmo::vtmWriter (vtm_writer.h:291-437)
+template <typename T, unsigned int Dim>
+class vtmWriter {
+ public:
+  // overlapth: -1 writes the whole stored block; otherwise blocks whose overlap
+  // exceeds it drop (overlap - overlapth) layers on each side
+  vtmWriter(std::string filename, BlockGeometry3D<T>& geo, int overlapth = -1)
+      : filename_(std::move(filename)) {
+    flbcpp::make_dir(dirname_);
+    flbcpp::make_dir(vtidirname_);
+    int ov = 0;
+    if (overlapth != -1 && overlapth < geo.getOverlap()) ov = geo.getOverlap() - overlapth;
+    vtis_.emplace_back(filename_, 0, geo.getVoxelSize(), geo.getMinCenter(),
+                       geo.getMesh() - Vector<int, Dim>(1), ov);
+  }
+  void addWriterSet(const AbstWriterSet& ws) {
+    int i = 0;
+    for (auto& v : vtis_) v.addWriter(ws.getWriter(i++));
+  }
+  template <typename... Args>
+  void addWriterSet(const AbstWriterSet& ws, const Args&... args) {
+    addWriterSet(ws);
+    addWriterSet(args...);
+  }
+  void WriteBinary() {
+    for (auto& v : vtis_) v.WriteBinary();
+    write_vtm(vtidirname_ + filename_ + ".vtm", [&](std::size_t i) {
+      return filename_ + "_B" + std::to_string(i) + ".vti";
+    });
+  }
+  void WriteBinary(int step) {
+    for (auto& v : vtis_) v.WriteBinary(step);
+    write_vtm(vtidirname_ + filename_ + std::to_string(step) + ".vtm", [&](std::size_t i) {
+      return filename_ + "_T" + std::to_string(step) + "_B" + std::to_string(i) + ".vti";
+    });
+  }
+
+ private:
+  template <typename F>
+  void write_vtm(const std::string& fullName, F&& vti_name) {
+    std::ofstream f(fullName, std::ios::trunc);
+    f << "<?xml version=\"1.0\"?>\n";
+    f << "<VTKFile type=\"vtkMultiBlockDataSet\" version=\"1.0\" "
+      << "byte_order=\"LittleEndian\">\n"
+      << "<vtkMultiBlockDataSet>\n";
+    for (std::size_t i = 0; i < vtis_.size(); ++i) {
+      f << "<Block index=\"" << i << "\" >\n";
+      f << "<DataSet index= \"0\" " << "file=\"" << vti_name(i) << "\">\n" << "</DataSet>\n";
+      f << "</Block>\n";
+    }
+    f << "</vtkMultiBlockDataSet>\n";
+    f << "</VTKFile>\n";
+  }
+  std::string dirname_ = "./vtkoutput/";
+  std::string vtidirname_ = "./vtkoutput/vtidata/";
+  std::string filename_;
+  std::vector<vtiManager<T, Dim>> vtis_;
+};
+}  // namespace vtmo

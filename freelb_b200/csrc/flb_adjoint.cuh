@@ -33,7 +33,7 @@ struct AdjParams {
   void* lam_out;        // lambda_t
   const void* q;        // Q_t: stored forward state with R_t = stream(Q_t)
   double* galpha;       // per-cell dJ/dalpha (FP64), own-cell layout
-  double* gscal;        // [0] dJ/dtau, [1] dJ/du_lid
+  double* gpart;        // per thread block: [2b] dJ/dtau, [2b+1] dJ/du_lid partial sums
 };
 
 // Transposed Jacobian of one cell.  f: R_t of the cell, mu in, lam out.
@@ -66,39 +66,66 @@ __device__ __forceinline__ void cell_vjp(int op, const R* f, const R* mu, R* lam
   forced_moments(f, alpha, rho, den, ux, uy, uz);
   const R u2 = ux * ux + uy * uy + uz * uz;
   const R fo = R(1) - R(0.5) * omega;
-  R sF = 0, sR = 0, sG = 0, sGa = 0, bx = 0, by = 0, bz = 0;
+  // The sums over i above need only the weighted moments of mu:
+  //   M0 = sum w_i mu_i, M1 = sum w_i mu_i c_i, P = sum w_i mu_i c_i c_i^T,
+  // since feq_i, G_i and their u-derivatives are polynomials in c_i:
+  //   sum mu_i feq_i = rho (M0 (1 - 3|u|^2/2) + 3 M1.u + 9/2 u.P.u)
+  //   sum mu_i w_i poly_i = 3 M1.u - 3 |u|^2 M0 + 9 u.P.u
+  //   b = 3 (w rho - fo alpha) M1 + (9 w rho - 18 fo alpha) P u - (3 w rho - 6 fo alpha) M0 u
+  // (w = omega, fo = 1 - omega/2).  Pair sums s and differences d of opposite
+  // directions carry all of it.
+  R sp[Q], dp[Q];
 #pragma unroll
-  for (int i = 0; i < Q; ++i) {
-    const R c0 = R(cx(i)), c1 = R(cy(i)), c2 = R(cz(i));
-    const R w = weight<R>(i);
-    const R cu = c0 * ux + c1 * uy + c2 * uz;
-    const R feq = w * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * u2);
-    const R poly = R(3) * cu - R(3) * u2 + R(9) * cu * cu;
-    const R G = -alpha * w * poly;
-    // w dfeq/du + (1 - w/2) dG/du
-    const R kf = omega * w * rho, kg = -fo * alpha * w;
-    const R t9 = R(9) * cu, t18 = R(18) * cu;
-    const R dx = kf * (R(3) * c0 + t9 * c0 - R(3) * ux) + kg * (R(3) * c0 - R(6) * ux + t18 * c0);
-    const R dy = kf * (R(3) * c1 + t9 * c1 - R(3) * uy) + kg * (R(3) * c1 - R(6) * uy + t18 * c1);
-    const R dz = kf * (R(3) * c2 + t9 * c2 - R(3) * uz) + kg * (R(3) * c2 - R(6) * uz + t18 * c2);
-    const R m = mu[i];
-    sF += m * feq;
-    sR += m * f[i];
-    sG += m * G;
-    sGa += m * (-w * poly);
-    bx += m * dx;
-    by += m * dy;
-    bz += m * dz;
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = mu[i] + mu[i + 1];
+    dp[i] = mu[i] - mu[i + 1];
   }
-  const R a = omega * sF / rho;
+  const R w0 = R(1) / R(3), wa = R(1) / R(18), wd = R(1) / R(36);
+  const R M0 = w0 * mu[0] + wa * ((sp[1] + sp[3]) + sp[5]) +
+               wd * (((sp[7] + sp[9]) + (sp[11] + sp[13])) + (sp[15] + sp[17]));
+  const R M1x = wa * dp[1] + wd * ((dp[7] + dp[9]) + (dp[13] + dp[15]));
+  const R M1y = wa * dp[3] + wd * ((dp[7] + dp[11]) + (dp[17] - dp[13]));
+  const R M1z = wa * dp[5] + wd * ((dp[9] + dp[11]) - (dp[15] + dp[17]));
+  const R Pxx = wa * sp[1] + wd * ((sp[7] + sp[9]) + (sp[13] + sp[15]));
+  const R Pyy = wa * sp[3] + wd * ((sp[7] + sp[11]) + (sp[13] + sp[17]));
+  const R Pzz = wa * sp[5] + wd * ((sp[9] + sp[11]) + (sp[15] + sp[17]));
+  const R Pxy = wd * (sp[7] - sp[13]);
+  const R Pxz = wd * (sp[9] - sp[15]);
+  const R Pyz = wd * (sp[11] - sp[17]);
+  const R Pux = Pxx * ux + Pxy * uy + Pxz * uz;
+  const R Puy = Pxy * ux + Pyy * uy + Pyz * uz;
+  const R Puz = Pxz * ux + Pyz * uy + Pzz * uz;
+  const R uPu = ux * Pux + uy * Puy + uz * Puz;
+  const R M1u = M1x * ux + M1y * uy + M1z * uz;
+  const R feq_sum = M0 * (R(1) - R(1.5) * u2) + R(3) * M1u + R(4.5) * uPu;  // sum mu feq / rho
+  const R poly_sum = R(3) * M1u - R(3) * u2 * M0 + R(9) * uPu;
+  const R sF = rho * feq_sum;
+  const R sGa = -poly_sum;
+  const R sG = alpha * sGa;
+  const R wr = omega * rho, fa = fo * alpha;
+  const R A = R(3) * (wr - fa), B = R(9) * wr - R(18) * fa, Cc = R(3) * wr - R(6) * fa;
+  const R bx = A * M1x + B * Pux - Cc * M0 * ux;
+  const R by = A * M1y + B * Puy - Cc * M0 * uy;
+  const R bz = A * M1z + B * Puz - Cc * M0 * uz;
+  R sR = 0;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) sR += mu[i] * f[i];
   const R inv_den = R(1) / den;
+  const R ub = bx * ux + by * uy + bz * uz;
+  // lambda_j = (1-w) mu_j + w sum mu feq / rho + (c_j - u).b / den
+  const R base = omega * feq_sum - ub * inv_den;
+  const R qx = bx * inv_den, qy = by * inv_den, qz = bz * inv_den;
+  const R c1 = R(1) - omega;
 #pragma unroll
   for (int j = 0; j < Q; ++j) {
-    const R cj = (R(cx(j)) - ux) * bx + (R(cy(j)) - uy) * by + (R(cz(j)) - uz) * bz;
-    lam[j] = (R(1) - omega) * mu[j] + a + cj * inv_den;
+    R cb = base;
+    if (cx(j) > 0) cb += qx; else if (cx(j) < 0) cb -= qx;
+    if (cy(j) > 0) cb += qy; else if (cy(j) < 0) cb -= qy;
+    if (cz(j) > 0) cb += qz; else if (cz(j) < 0) cb -= qz;
+    lam[j] = c1 * mu[j] + cb;
   }
   gtau += -double(omega) * double(omega) * (double(sF) - double(sR) - 0.5 * double(sG));
-  galpha += double(-(bx * ux + by * uy + bz * uz) * R(0.5) * inv_den) + double(fo) * double(sGa);
+  galpha += double(-ub * R(0.5) * inv_den) + double(fo) * double(sGa);
 }
 
 // One backward step over a single block: lam_out = J_C^T S^T lam_in.
@@ -154,11 +181,21 @@ __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const 
     }
   }
   }
+  // Thread block b adds its sums to its own slots (same grid every step, one
+  // stream): no atomics, and the final sum over blocks has a fixed order.
   gtau = warp_sum(gtau);
   gulid = warp_sum(gulid);
-  if ((threadIdx.x & 31) == 0) {
-    if (gtau != 0.0) atomicAdd(a.gscal + 0, gtau);
-    if (gulid != 0.0) atomicAdd(a.gscal + 1, gulid);
+  __shared__ double red[2][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wid] = gtau;
+    red[1][wid] = gulid;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    double v = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+    a.gpart[2 * blockIdx.x + threadIdx.x] += v;
   }
 }
 

@@ -21,7 +21,9 @@
 #include <vector>
 
 #include "../../include/flb.h"
+#include "../../include/flb_vtk.h"
 #include "flb_adjoint.cuh"
+#include "flb_vtk.cuh"
 
 using namespace flb;
 
@@ -93,6 +95,7 @@ struct flb_lattice {
   void* stage = nullptr;
   size_t stage_bytes = 0;
   double* uprev = nullptr;
+  uint8_t* d_lut = nullptr;  // op of every flag value
   StepParams sp{};
   // multi-block launch data
   BlockEntry* d_blocks = nullptr;
@@ -101,6 +104,7 @@ struct flb_lattice {
   int table_vec = 0;
   HaloCopy* d_halo = nullptr;
   long long nhalo = 0;
+  int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
   int ctas_per_sm = 0;
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
@@ -114,6 +118,8 @@ struct flb_lattice {
   std::vector<void*> adj_seg;   // recomputed Q_{t0+1} .. Q_{t0+k-1}
   void* adj_lam[2] = {nullptr, nullptr};
   double* adj_galpha = nullptr;
+  double* adj_gpart = nullptr;  // per-thread-block dJ/dtau, dJ/du_lid sums
+  size_t adj_gpart_n = 0;
 };
 
 namespace {
@@ -192,6 +198,7 @@ void build_params(flb_lattice* h) {
     p.keys[t] = d.task_keys[t];
     p.ops[t] = d.task_ops[t];
   }
+  p.op_lut = h->d_lut;
   const bool dbl = d.storage == FLB_STORAGE_FP64;
   p.omega = arith_omega(d, d.omega);
   const double cs = dbl ? d.smagorinsky : double(float(d.smagorinsky));
@@ -212,6 +219,7 @@ void build_params(flb_lattice* h) {
   // while leaving headroom to |f - w| = 64.
   p.scale = 1024.0f;
   p.inv_scale = 1.0f / 1024.0f;
+  p.rho0 = float(d.rho0);
 }
 
 // Cells per thread of the pull kernel (launch parameter; defaults are the
@@ -224,6 +232,22 @@ bool vec_allowed(int storage, int v) {
 
 Geom geom_of(const HostBlock& b) {
   return Geom{b.L.nx, b.L.ny, b.L.nz, b.L.pitch, b.L.plane, b.base};
+}
+
+// Op lookup table: for every flag value, the op of the first task whose key
+// shares a bit with it (src/utils/tmp.h:283-309).
+int upload_op_lut(flb_lattice* h) {
+  uint8_t lut[256];
+  for (int v = 0; v < 256; ++v) {
+    lut[v] = FLB_OP_NONE;
+    for (int t = 0; t < h->desc.ntasks; ++t)
+      if (v & h->desc.task_keys[t]) {
+        lut[v] = h->desc.task_ops[t];
+        break;
+      }
+  }
+  FLB_CUDA(cudaMemcpy(h->d_lut, lut, sizeof lut, cudaMemcpyHostToDevice));
+  return FLB_OK;
 }
 
 // Block table for the tile kernel (rebuilt when tile_y changes).
@@ -302,12 +326,13 @@ int build_halo(flb_lattice* h) {
           const Geom gn = geom_of(n);
           const int l[3] = {lx, ly, lz};
           const int m[3] = {b.L.nx, b.L.ny, b.L.nz};
-          for (int i = 1; i < Q; ++i) {
+          const bool full = h->halo_mode == FLB_HALO_FULL;
+          for (int i = full ? 0 : 1; i < Q; ++i) {
             const int c[3] = {cx(i), cy(i), cz(i)};
             bool cross = false;
             for (int a = 0; a < 3; ++a)
               if ((l[a] == 0 && c[a] > 0) || (l[a] == m[a] - 1 && c[a] < 0)) cross = true;
-            if (!cross) continue;
+            if (!cross && !full) continue;
             HaloCopy r;
             r.dir = i;
             r.dst = host_wrap_src(gb, lx, ly, lz, i);
@@ -316,6 +341,8 @@ int build_halo(flb_lattice* h) {
           }
         }
   }
+  if (h->d_halo) cudaFree(h->d_halo);
+  h->d_halo = nullptr;
   h->nhalo = (long long)recs.size();
   if (!recs.empty()) {
     FLB_CUDA(cudaMalloc((void**)&h->d_halo, recs.size() * sizeof(HaloCopy)));
@@ -592,7 +619,8 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
   if ((e = cudaMalloc((void**)&h->flags, ds)) != cudaSuccess ||
       (e = cudaMalloc(&h->rho, ds * h->real_bytes)) != cudaSuccess ||
       (e = cudaMalloc(&h->vel, 3 * ds * h->real_bytes)) != cudaSuccess ||
-      (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess)
+      (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&h->d_lut, 256)) != cudaSuccess)
     return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
   if (desc->model == FLB_MODEL_BRINKMAN) {
     if ((e = cudaMalloc(&h->alpha, ds * h->real_bytes)) != cudaSuccess ||
@@ -600,6 +628,11 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
       return cleanup(fail(FLB_ERR_OOM, "cudaMalloc alpha: %s", cudaGetErrorString(e)));
   }
   build_params(h);
+  if (int rc0 = upload_op_lut(h)) return cleanup(rc0);
+  for (const HostBlock& b : h->blocks)
+    if ((long long)(b.L.pitch) * b.L.ny * b.L.nz >= (1LL << 32))
+      return cleanup(fail(FLB_ERR_INVALID, "block of %lld padded cells exceeds 2^32",
+                          (long long)(b.L.pitch) * b.L.ny * b.L.nz));
   if (mode == FLB_BLOCKS_HALO) {
     int rc = build_halo(h);
     if (rc) return cleanup(rc);
@@ -712,7 +745,8 @@ int flb_destroy(flb_lattice* h) {
   flb_adjoint_release(h);
   if (h->alpha) cudaFree(h->alpha);
   for (void* p : {h->pops[0], h->pops[1], (void*)h->flags, h->rho, h->vel, (void*)h->acc,
-                  h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo})
+                  h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo,
+                  (void*)h->d_lut})
     if (p) cudaFree(p);
   delete h;
   return FLB_OK;
@@ -738,7 +772,7 @@ int flb_set_tasks(flb_lattice* h, int ntasks, const uint8_t* keys, const uint8_t
   h->sp.src = keep.src;
   h->sp.dst = keep.dst;
   drop_graphs(h);
-  return FLB_OK;
+  return upload_op_lut(h);
 }
 
 int flb_block_count(const flb_lattice* h, int* n) {
@@ -751,6 +785,19 @@ int flb_halo_count(const flb_lattice* h, long long* n) {
   if (!h || !n) return fail(FLB_ERR_INVALID, "null argument");
   *n = h->nhalo;
   return FLB_OK;
+}
+
+int flb_set_halo_mode(flb_lattice* h, int mode) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (mode != FLB_HALO_NORMAL && mode != FLB_HALO_FULL)
+    return fail(FLB_ERR_INVALID, "unknown halo mode %d", mode);
+  if (h->mode != FLB_BLOCKS_HALO)
+    return fail(FLB_ERR_STATE, "halo mode applies to FLB_BLOCKS_HALO handles");
+  if (mode == h->halo_mode) return FLB_OK;
+  FLB_CUDA(cudaDeviceSynchronize());  // the old records may be in use by queued steps
+  h->halo_mode = mode;
+  drop_graphs(h);
+  return build_halo(h);
 }
 
 int flb_memory_bytes(const flb_lattice* h, size_t* bytes) {
@@ -1082,6 +1129,9 @@ int flb_adjoint_release(flb_lattice* h) {
     }
   if (h->adj_galpha) cudaFree(h->adj_galpha);
   h->adj_galpha = nullptr;
+  if (h->adj_gpart) cudaFree(h->adj_gpart);
+  h->adj_gpart = nullptr;
+  h->adj_gpart_n = 0;
   h->adj_T = h->adj_k = 0;
   return FLB_OK;
 }
@@ -1151,9 +1201,8 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
       return fail(FLB_ERR_OOM, "recompute slot (%zu bytes): %s", qbytes, cudaGetErrorString(e));
     h->adj_seg.push_back(p);
   }
-  double* gscal = h->acc + 5;  // [0] tau, [1] u_lid
   double* jacc = h->acc + 4;
-  FLB_CUDA(cudaMemsetAsync(h->acc + 4, 0, 3 * sizeof(double), st));
+  FLB_CUDA(cudaMemsetAsync(h->acc + 4, 0, sizeof(double), st));
   // seed lambda_T = dJ/dR_T and the direct dJ/dalpha term
   k_objective<R, R><<<grid_1d(b.padded()), 256, 0, st>>>(
       b.L, geom_of(b), static_cast<const R*>(h->pops[h->cur]), h->sp,
@@ -1163,9 +1212,18 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
   const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
   const dim3 block(32 * h->tile_y);
   const dim3 grid(unsigned((chunks + block.x - 1) / block.x));
+  const size_t npart = 2 * size_t(grid.x);
+  if (h->adj_gpart_n < npart) {
+    if (h->adj_gpart) cudaFree(h->adj_gpart);
+    h->adj_gpart = nullptr;
+    h->adj_gpart_n = 0;
+    FLB_CUDA(cudaMalloc((void**)&h->adj_gpart, npart * sizeof(double)));
+    h->adj_gpart_n = npart;
+  }
+  FLB_CUDA(cudaMemsetAsync(h->adj_gpart, 0, npart * sizeof(double), st));
   AdjParams a{};
   a.galpha = h->adj_galpha;
-  a.gscal = gscal;
+  a.gpart = h->adj_gpart;
   const int T = h->adj_T;
   const int nseg = (T + k - 1) / k;
   for (int sgi = nseg - 1; sgi >= 0; --sgi) {
@@ -1186,8 +1244,9 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
     }
     FLB_CUDA(cudaGetLastError());
   }
-  double sc[2] = {0, 0};
-  FLB_CUDA(cudaMemcpyAsync(sc, gscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  std::vector<double> part(npart);
+  FLB_CUDA(cudaMemcpyAsync(part.data(), h->adj_gpart, npart * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
   if (dJ_dalpha) {
     const LayoutParams& L = b.L;
     FLB_CUDA(cudaMemcpy2DAsync(dJ_dalpha, L.nx * sizeof(double), h->adj_galpha,
@@ -1195,6 +1254,11 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
                                size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
   }
   FLB_CUDA(cudaStreamSynchronize(st));
+  double sc[2] = {0, 0};
+  for (size_t b2 = 0; b2 < npart; b2 += 2) {
+    sc[0] += part[b2];
+    sc[1] += part[b2 + 1];
+  }
   if (dJ_dtau) *dJ_dtau = sc[0];
   if (dJ_dulid) *dJ_dulid = sc[1];
   return FLB_OK;
@@ -1214,6 +1278,92 @@ int flb_adjoint_backward(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau, dou
   if (h->desc.storage == FLB_STORAGE_FP64)
     return adjoint_backward_t<double>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
   return adjoint_backward_t<float>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// VTK DataArray bodies of device fields (flb_vtk.h)
+
+template <typename R, typename O>
+static int vtk_launch(const VtkArgs& a, unsigned* d_out, cudaStream_t st) {
+  const long long groups = (a.nbytes + 2) / 3;
+  long long blocks = (groups + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148LL * 64) blocks = 148LL * 64;
+  k_vtk_base64<R, O><<<unsigned(blocks), 256, 0, st>>>(a, d_out);
+  FLB_CUDA(cudaGetLastError());
+  return FLB_OK;
+}
+
+extern "C" {
+
+int flb_vtk_field_base64(flb_lattice* h, int block, int field, int overlap, int out_dtype,
+                         int map, double scale, double offset, char* out, size_t cap,
+                         size_t* len, void* stream) {
+  if (!h || !len) return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: null argument");
+  if (block < 0 || block >= int(h->blocks.size()))
+    return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: block %d of %d", block,
+                int(h->blocks.size()));
+  const HostBlock& b = h->blocks[block];
+  const LayoutParams& L = b.L;
+  if (overlap < 0 || 2 * overlap >= L.nx || 2 * overlap >= L.ny || 2 * overlap >= L.nz)
+    return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: overlap %d too large", overlap);
+  const bool dbl = h->desc.storage == FLB_STORAGE_FP64;
+  const size_t rsize = dbl ? 8 : 4;
+  VtkArgs a{};
+  a.comp_stride = h->dstride;
+  a.pitch = L.pitch;
+  a.plane = L.plane;
+  a.sx = L.nx - 2 * overlap;
+  a.sy = L.ny - 2 * overlap;
+  a.sz = L.nz - 2 * overlap;
+  a.ox = a.oy = a.oz = overlap;
+  a.ncomp = 1;
+  a.map = map ? 1 : 0;
+  a.scale = scale;
+  a.offset = offset;
+  size_t osize = 1;
+  if (field == FLB_VTK_FLAG) {
+    a.src = h->flags + b.base;
+    osize = 1;
+  } else {
+    if (out_dtype != FLB_DTYPE_F32 && out_dtype != FLB_DTYPE_F64)
+      return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: out_dtype %d", out_dtype);
+    osize = out_dtype == FLB_DTYPE_F64 ? 8 : 4;
+    const char* base = nullptr;
+    if (field == FLB_FIELD_RHO) base = static_cast<const char*>(h->rho);
+    else if (field == FLB_FIELD_VELOCITY) base = static_cast<const char*>(h->vel), a.ncomp = 3;
+    else if (field == FLB_FIELD_ALPHA) base = static_cast<const char*>(h->alpha);
+    else return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: unknown field %d", field);
+    if (!base) return fail(FLB_ERR_STATE, "flb_vtk_field_base64: field %d not allocated", field);
+    a.src = base + size_t(b.base) * rsize;
+  }
+  const long long nelem = (long long)a.sx * a.sy * a.sz * a.ncomp;
+  a.nbytes = nelem * (long long)osize;
+  const size_t nchar = 8 + 4 * size_t((a.nbytes + 2) / 3);
+  *len = nchar;
+  if (!out) return FLB_OK;
+  if (cap < nchar)
+    return fail(FLB_ERR_INVALID, "flb_vtk_field_base64: buffer of %zu characters, need %zu", cap,
+                nchar);
+  cudaStream_t st = as_stream(stream);
+  unsigned* d_out = nullptr;
+  FLB_CUDA(cudaMalloc((void**)&d_out, (nchar + 3) & ~size_t(3)));
+  int rc = FLB_OK;
+  if (field == FLB_VTK_FLAG) rc = vtk_launch<uint8_t, uint8_t>(a, d_out, st);
+  else if (dbl && osize == 8) rc = vtk_launch<double, double>(a, d_out, st);
+  else if (dbl) rc = vtk_launch<double, float>(a, d_out, st);
+  else if (osize == 8) rc = vtk_launch<float, double>(a, d_out, st);
+  else rc = vtk_launch<float, float>(a, d_out, st);
+  cudaError_t e = cudaSuccess;
+  if (rc == FLB_OK) e = cudaMemcpyAsync(out, d_out, nchar, cudaMemcpyDeviceToHost, st);
+  if (rc == FLB_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d_out);
+  if (rc) return rc;
+  if (e != cudaSuccess)
+    return fail(FLB_ERR_CUDA, "flb_vtk_field_base64: %s", cudaGetErrorString(e));
+  return FLB_OK;
 }
 
 }  // extern "C"

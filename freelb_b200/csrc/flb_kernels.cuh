@@ -34,25 +34,19 @@ struct StepParams {
   int ntasks;
   uint8_t keys[8];
   uint8_t ops[8];
+  const uint8_t* op_lut;  // op of every flag value (device, 256 entries)
   double omega;       // 1/tau, already rounded to the arithmetic type
   double cs_coeff;    // Cs^2 * 9 * 2 * sqrt(2) (LES)
   double s_over_norm[Q];  // MRT: s_k / |M_k|^2
   float shift[Q];     // FP16S: rho0 * w_i
   float scale, inv_scale;
+  float rho0;         // FP16S: density of the shift
 };
 
-// First task whose key shares a bit with the flag (src/utils/tmp.h:283-309).
+// First task whose key shares a bit with the flag (src/utils/tmp.h:283-309),
+// tabulated on the host for all 256 flag values.
 __device__ __forceinline__ int select_op(const StepParams& p, uint8_t flag) {
-  int op = 0;
-  bool found = false;
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    if (!found && t < p.ntasks && (flag & p.keys[t])) {
-      op = p.ops[t];
-      found = true;
-    }
-  }
-  return op;
+  return __ldg(p.op_lut + flag);
 }
 
 enum : int { OP_NONE = 0, OP_BULK = 1, OP_BB = 2, OP_MBB = 3, OP_FIELD_BGK = 4 };

@@ -105,8 +105,10 @@ struct Storage<__half, float> {
   __device__ static __forceinline__ float load(const __half* p, float shift, float inv_scale) {
     return fmaf(__half2float(*p), inv_scale, shift);
   }
+  // scale is a power of two, so (v - shift) * scale == v * scale - shift * scale
+  // exactly before the single rounding of the fused multiply-add.
   __device__ static __forceinline__ void store(__half* p, float v, float shift, float scale) {
-    *p = __float2half_rn((v - shift) * scale);
+    *p = __float2half_rn(fmaf(v, scale, -shift * scale));
   }
 };
 

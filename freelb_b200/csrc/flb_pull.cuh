@@ -68,11 +68,13 @@ __device__ __forceinline__ void vstore(S* p, const R* in, float shift, float sca
   } else if constexpr (std::is_same<S, double>::value && V == 2) {
     *reinterpret_cast<double2*>(p) = make_double2(in[0], in[1]);
   } else if constexpr (std::is_same<S, __half>::value && V == 2) {
-    const __half2 a = __floats2half2_rn((in[0] - shift) * scale, (in[1] - shift) * scale);
+    const float ns = -shift * scale;  // exact: scale is a power of two
+    const __half2 a = __floats2half2_rn(fmaf(in[0], scale, ns), fmaf(in[1], scale, ns));
     *reinterpret_cast<unsigned*>(p) = *reinterpret_cast<const unsigned*>(&a);
   } else if constexpr (std::is_same<S, __half>::value && V == 4) {
-    const __half2 a = __floats2half2_rn((in[0] - shift) * scale, (in[1] - shift) * scale);
-    const __half2 b = __floats2half2_rn((in[2] - shift) * scale, (in[3] - shift) * scale);
+    const float ns = -shift * scale;
+    const __half2 a = __floats2half2_rn(fmaf(in[0], scale, ns), fmaf(in[1], scale, ns));
+    const __half2 b = __floats2half2_rn(fmaf(in[2], scale, ns), fmaf(in[3], scale, ns));
     uint2 v;
     v.x = *reinterpret_cast<const unsigned*>(&a);
     v.y = *reinterpret_cast<const unsigned*>(&b);
@@ -224,10 +226,228 @@ __device__ __forceinline__ void collide_chunk(const StepParams& p, const Geom& g
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP16S storage: populations stay packed (V halves per direction) from the
+// load to the store, and bulk BGK cells collide on the stored deviations.
+//
+// The stored value is H_i = (f_i - w_i rho0) S, S = 2^10.  With
+// delta = rho - rho0 = sum_i H_i / S and u = sum_i c_i H_i / (S rho) (the
+// weights w_i carry no momentum), BGK f'_i = omega feq_i + (1 - omega) f_i with
+// feq_i = w_i rho (1 + g_i) (equilibrium::SecondOrder, src/lbm/equilibrium.ur.h:
+// 166-215) reads, on deviations,
+//   H'_i = (1 - omega) H_i + omega S w_i (delta + rho g_i),
+//   g_i = k_i + k_i^2 / 2 - 3 |u|^2 / 2,  k_i = 3 c_i . u,
+// in FP32 without forming f_i = w_i rho0 + H_i / S: no shift or scale per
+// population and no cancellation against w_i rho0.  Other ops convert to f_i,
+// apply the generic operator and convert back; cells without an op keep their
+// stored bits.
+
+template <int V> struct HWord;
+template <> struct HWord<2> { using type = unsigned; };
+template <> struct HWord<4> { using type = uint2; };
+
+template <int V>
+__device__ __forceinline__ typename HWord<V>::type hload(const __half* p) {
+  if constexpr (V == 4) return __ldg(reinterpret_cast<const uint2*>(p));
+  else return __ldg(reinterpret_cast<const unsigned*>(p));
+}
+template <int V>
+__device__ __forceinline__ void hstore(__half* p, const typename HWord<V>::type& w) {
+  if constexpr (V == 4) *reinterpret_cast<uint2*>(p) = w;
+  else *reinterpret_cast<unsigned*>(p) = w;
+}
+__device__ __forceinline__ unsigned hscalar(const __half* p) {
+  return __ldg(reinterpret_cast<const unsigned short*>(p));
+}
+// 32-bit part holding halves k and k+1 (k even) of a word
+__device__ __forceinline__ unsigned& hpart(unsigned& w, int) { return w; }
+__device__ __forceinline__ unsigned& hpart(uint2& w, int k) { return k < 2 ? w.x : w.y; }
+// half k of the word := bits h (low 16)
+template <typename W>
+__device__ __forceinline__ void hset(W& w, int k, unsigned h) {
+  unsigned& q = hpart(w, k);
+  q = (k & 1) ? __byte_perm(q, h, 0x5410) : __byte_perm(q, h, 0x3254);
+}
+// [a.hi, b.lo]: the halves on both sides of a 32-bit boundary
+__device__ __forceinline__ unsigned hcross(unsigned a, unsigned b) {
+  return __byte_perm(a, b, 0x5432);
+}
+// source chunk shifted by one cell: v = own chunk, w = chunk before (prev) or after (next)
+__device__ __forceinline__ unsigned hsplice_prev(unsigned w, unsigned v) { return hcross(w, v); }
+__device__ __forceinline__ unsigned hsplice_next(unsigned v, unsigned w) { return hcross(v, w); }
+__device__ __forceinline__ uint2 hsplice_prev(uint2 w, uint2 v) {
+  return make_uint2(hcross(w.y, v.x), hcross(v.x, v.y));
+}
+__device__ __forceinline__ uint2 hsplice_next(uint2 v, uint2 w) {
+  return make_uint2(hcross(v.x, v.y), hcross(v.y, w.x));
+}
+
+// The V post-stream words of chunk x0 of row (y, z): the same loads and edge
+// rules as gather_chunk (SIGN = +1), without conversion.
+template <int V>
+__device__ __forceinline__ void gather_words(const __half* __restrict__ arr, long long dstride,
+                                             const Geom& g, int x0, int y, int z,
+                                             typename HWord<V>::type (&h)[Q]) {
+  using W = typename HWord<V>::type;
+  const bool inner_row = y > 0 && z > 0 && y < g.ny - 1 && z < g.nz - 1;
+  if (inner_row) {
+    const int xprev = x0 >= V ? x0 - V : x0;
+    const int xnext = x0 + V < g.nx ? x0 + V : x0;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const __half* rowp = arr + i * dstride + g.base + (long long)(y - cy(i)) * g.pitch +
+                           (long long)(z - cz(i)) * g.plane;
+      const W v = hload<V>(rowp + x0);
+      if (cx(i) == 0) {
+        h[i] = v;
+      } else if (cx(i) > 0) {
+        h[i] = hsplice_prev(hload<V>(rowp + xprev), v);
+      } else {
+        h[i] = hsplice_next(v, hload<V>(rowp + xnext));
+      }
+    }
+    if (x0 == 0) {
+#pragma unroll
+      for (int i = 1; i < Q; ++i)
+        if (cx(i) > 0)
+          hset(h[i], 0, hscalar(arr + i * dstride + wrap_off(g, 0, y, z, -cx(i), -cy(i), -cz(i))));
+    }
+    const int klast = g.nx - 1 - x0;
+    if (klast >= 0 && klast < V) {
+#pragma unroll
+      for (int k = 0; k < V; ++k)
+        if (k == klast) {
+#pragma unroll
+          for (int i = 1; i < Q; ++i)
+            if (cx(i) < 0)
+              hset(h[i], k,
+                   hscalar(arr + i * dstride +
+                           wrap_off(g, g.nx - 1, y, z, -cx(i), -cy(i), -cz(i))));
+        }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) h[i] = W{};
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const int x = min(x0 + k, g.nx - 1);
+#pragma unroll
+      for (int i = 0; i < Q; ++i)
+        hset(h[i], k, hscalar(arr + i * dstride + wrap_off(g, x, y, z, -cx(i), -cy(i), -cz(i))));
+    }
+  }
+}
+
+// BGK on deviations (see above); H[] in and out in units of the stored value.
+__device__ __forceinline__ void bgk_deviation(float (&H)[Q], float omega, float rho0,
+                                              float scale, float inv_scale) {
+  float sp[Q], df[Q];  // pair sums / differences, index of the first of the pair
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = H[i] + H[i + 1];
+    df[i] = H[i] - H[i + 1];
+  }
+  const float sum = ((H[0] + sp[1]) + (sp[3] + sp[5])) + ((sp[7] + sp[9]) + (sp[11] + sp[13])) +
+                    ((sp[15] + sp[17]));
+  const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
+  const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
+  const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
+  const float delta = sum * inv_scale;
+  const float rho = rho0 + delta;
+  const float ir = __fdividef(inv_scale, rho);  // 1 / (S rho)
+  const float ux = mx * ir, uy = my * ir, uz = mz * ir;
+  const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+  const float c1 = 1.0f - omega;
+  const float W0 = omega * scale * (1.0f / 3.0f);
+  const float W1 = omega * scale * (1.0f / 18.0f);
+  const float W2 = omega * scale * (1.0f / 36.0f);
+  const float d0 = W0 * delta, d1 = W1 * delta, d2 = W2 * delta;
+  const float r0 = W0 * rho, r1 = W1 * rho, r2 = W2 * rho;
+  const float k1 = 3.0f * ux, k3 = 3.0f * uy, k5 = 3.0f * uz;
+  float k[Q];
+  k[1] = k1;
+  k[3] = k3;
+  k[5] = k5;
+  k[7] = k1 + k3;
+  k[9] = k1 + k5;
+  k[11] = k3 + k5;
+  k[13] = k1 - k3;
+  k[15] = k1 - k5;
+  k[17] = k3 - k5;
+  H[0] = fmaf(r0, q, fmaf(c1, H[0], d0));
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float dw = i < 7 ? d1 : d2;
+    const float rw = i < 7 ? r1 : r2;
+    const float e = fmaf(0.5f * k[i], k[i], q);
+    H[i] = fmaf(rw, e + k[i], fmaf(c1, H[i], dw));
+    H[i + 1] = fmaf(rw, e - k[i], fmaf(c1, H[i + 1], dw));
+  }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void collide_deviation(const StepParams& p, int op, float (&H)[Q],
+                                                  long long cell, float omega) {
+  if (op == OP_NONE) return;
+  if constexpr (MODEL == MODEL_BGK) {
+    if (op == OP_BULK) {
+      bgk_deviation(H, omega, p.rho0, p.scale, p.inv_scale);
+      return;
+    }
+  }
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = fmaf(H[i], p.inv_scale, p.shift[i]);
+  apply_op<float, MODEL>(p, op, f, cell, omega);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) H[i] = fmaf(f[i], p.scale, -p.shift[i] * p.scale);
+}
+
+// One FP16S chunk, cells processed in pairs (the two halves of a 32-bit part).
+template <int MODEL, int V>
+__device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom& g, float omega,
+                                                int x0, int y, int z) {
+  using W = typename HWord<V>::type;
+  const __half* __restrict__ src = static_cast<const __half*>(p.src);
+  __half* __restrict__ dst = static_cast<__half*>(p.dst);
+  W h[Q];
+  gather_words<V>(src, p.dstride, g, x0, y, z, h);
+  const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
+  uint8_t fl[V];
+  load_flags<V>(p.flags + cell0, fl);
+#pragma unroll
+  for (int k = 0; k < V; k += 2) {
+    const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
+    if (opa == OP_NONE && opb == OP_NONE) continue;
+    float a[Q], b[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const unsigned q = hpart(h[i], k);
+      const __half2 h2 = *reinterpret_cast<const __half2*>(&q);
+      a[i] = __low2float(h2);
+      b[i] = __high2float(h2);
+    }
+    collide_deviation<MODEL>(p, opa, a, cell0 + k, omega);
+    collide_deviation<MODEL>(p, opb, b, cell0 + k + 1, omega);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      // a cell without an op round-trips exactly (half -> float -> half)
+      const __half2 r = __floats2half2_rn(a[i], b[i]);
+      hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
+}
+
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
 template <typename S, typename R, int MODEL, int V>
 __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R omega, int lane,
                                            int x0, int y, int z) {
+  if constexpr (std::is_same<S, __half>::value && V >= 2) {
+    pull_chunk_half<MODEL, V>(p, g, omega, x0, y, z);
+    return;
+  }
   const S* __restrict__ src = static_cast<const S*>(p.src);
   S* __restrict__ dst = static_cast<S*>(p.dst);
   R vals[Q][V];
@@ -248,15 +468,20 @@ __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R
 
 // Chunk q of a block (V cells, counted over the padded rows: pitch / V chunks
 // per row) -> (x0, y, z); false for chunks in the row padding or past the end.
+// 32-bit arithmetic: a block holds fewer than 2^32 chunks (checked at creation).
 template <int V>
 __device__ __forceinline__ bool chunk_coords(const Geom& g, long long q, int& x0, int& y,
                                              int& z) {
-  const int cpr = g.pitch / V;
-  const long long row = q / cpr;
-  x0 = int(q - row * cpr) * V;
-  y = int(row % g.ny);
-  z = int(row / g.ny);
-  return z < g.nz && x0 < g.nx;
+  const unsigned cpr = unsigned(g.pitch / V);
+  const unsigned total = cpr * unsigned(g.ny) * unsigned(g.nz);
+  if (q >= (long long)total) return false;
+  const unsigned uq = unsigned(q);
+  const unsigned row = uq / cpr;
+  x0 = int(uq - row * cpr) * V;
+  const unsigned zz = row / unsigned(g.ny);
+  y = int(row - zz * unsigned(g.ny));
+  z = int(zz);
+  return x0 < g.nx;
 }
 
 // Single block: one thread per chunk; consecutive threads take consecutive

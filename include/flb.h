@@ -144,6 +144,15 @@ FLB_API int flb_block_count(const flb_lattice* lat, int* nblocks);
 /* number of halo copy records (overlap cells fed by a neighbour) */
 FLB_API int flb_halo_count(const flb_lattice* lat, long long* nrecords);
 
+/* Halo exchange of an FLB_BLOCKS_HALO handle.  FLB_HALO_NORMAL (default):
+ * NormalCommunicate, the directions crossing into the block.  FLB_HALO_FULL:
+ * NormalFullCommunicate / NormalAllCommunicate (block_lattice.hh:1448-1503,
+ * 1687-1720): all 19 populations of every overlap cell from its owner (with
+ * one overlap layer the first layer is all of them, so the two coincide). */
+#define FLB_HALO_NORMAL 0
+#define FLB_HALO_FULL 1
+FLB_API int flb_set_halo_mode(flb_lattice* lat, int mode);
+
 /* Rebind the per-flag task list and the bulk model (the NSTask type of
  * ApplyCellDynamics<NSTask>, src/utils/tmp.h:283-309): tasks are tried in order,
  * a cell takes the op of the first task whose key shares a bit with its flag. */

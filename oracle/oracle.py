@@ -192,7 +192,8 @@ def ref_binary(dtype=np.float32):
 
 
 def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float32,
-                  blockfile=None, threads=None, outdir=None, alpha=None):
+                  blockfile=None, threads=None, outdir=None, alpha=None, fields=None,
+                  poststream=None):
     """Run the reference's own CPU path; returns (dict of arrays, mlups)."""
     exe = ref_binary(dtype)
     if exe is None:
@@ -208,6 +209,12 @@ def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float3
         afile = os.path.join(tempfile.mkdtemp(), "alpha.bin")
         np.ascontiguousarray(alpha, dtype=dtype).tofile(afile)
         env["FLB_ALPHA_FILE"] = afile
+    if fields is not None:  # (rho[N], u[N, 3]) replacing the RHO and VELOCITY fields
+        ffile = os.path.join(tempfile.mkdtemp(), "fields.bin")
+        np.concatenate([np.ravel(fields[0]), np.ravel(fields[1])]).astype(dtype).tofile(ffile)
+        env["FLB_FIELDS_FILE"] = ffile
+    if poststream is not None:  # wall kind 1..5 of the post-stream managers
+        env["FLB_POSTSTREAM_BB"] = str(int(poststream))
     args = [exe, model, str(ni), repr(float(tau)), repr(float(ulid)), str(steps), str(warmup),
             outdir, repr(float(cs))]
     if blockfile:
@@ -320,3 +327,124 @@ class MultiBlock:
 
     def rhou_fields(self, key=2):
         return [lat.rhou_fields(key) for lat in self.lats]
+
+
+BB_KINDS = ("normal", "movingwall", "anti_simple", "anti_o1", "anti_o2", "anti_pressure")
+
+
+def poststream_bb(lat, cell_flag, void_flag, kind="normal"):
+    """Post-stream halfway bounce-back of one BBLikeFixedBlockBdManager
+    (src/boundary/boundary.h:86-140) on a restated lattice.  For every inner
+    cell with `cell_flag` and every direction k whose neighbour x + c_k has
+    `void_flag` (basic_boundary.h:196-211), the outflow j = opp(k) is set from
+    prev = getPrevious(k)(x) = R_k(x + Delta_k mod N) (field.h:645-656) and the
+    cell's RHO and VELOCITY fields (bounce_back_boundary.h:167-256):
+        normal         R_j = prev
+        movingwall     R_j = prev + 2 InvCs2 w_j rho (u . c_j)
+        anti_simple    R_j = 2 rho w_j - prev
+        anti_o1        R_j = 2 feq1_j(rho, u) - prev
+        anti_o2        R_j = 2 feq2_j(rho, u, |u|^2) - prev
+        anti_pressure  R_j = 2 rho w_j (1 + (uw . c_j)^2 InvCs4 / 2
+                                        - |uw|^2 InvCs2 / 2) - prev,
+                       uw = u + (u - u(x + c_k)) / 2.
+    The arithmetic follows the reference expressions term by term."""
+    if kind is True or kind is False:  # moving flag of the two-kind form
+        kind = "movingwall" if kind else "normal"
+    if kind not in BB_KINDS:
+        raise ValueError(f"unknown bounce-back kind {kind!r}")
+    nx, ny, nz, N = lat.nx, lat.ny, lat.nz, lat.N
+    R = lat.pops.reshape(19, N)
+    f = lat.flags.reshape(nz, ny, nx)
+    inner = np.zeros_like(f, dtype=bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    cells = np.flatnonzero((inner & ((f & cell_flag) != 0)).reshape(-1))
+    x = cells % nx
+    y = (cells // nx) % ny
+    z = cells // (nx * ny)
+    T = lat.dtype.type
+    U = lat.u.reshape(-1, 3)
+    opp = [0] + [i + 1 if i % 2 else i - 1 for i in range(1, 19)]
+
+    def dot(u, c):
+        return (u[:, 0] * T(c[0]) + u[:, 1] * T(c[1])) + u[:, 2] * T(c[2])
+
+    def norm2(u):
+        return (u[:, 0] * u[:, 0] + u[:, 1] * u[:, 1]) + u[:, 2] * u[:, 2]
+
+    for k in range(1, 19):
+        cxk, cyk, czk = (int(v) for v in C[k])
+        nb = (x + cxk) + nx * ((y + cyk) + ny * (z + czk))
+        sel = (lat.flags[nb] & void_flag) != 0
+        if not sel.any():
+            continue
+        xs = cells[sel]
+        d = cxk + cyk * nx + czk * nx * ny
+        prev = R[k, (xs + d) % N].copy()
+        j = opp[k]
+        w = T(1) / T(3) if j == 0 else (T(1) / T(18) if j < 7 else T(1) / T(36))
+        rho = lat.rho[xs]
+        u = U[xs]
+        if kind == "normal":
+            val = prev
+        elif kind == "movingwall":
+            val = prev + T(2) * T(3) * w * rho * dot(u, C[j])
+        elif kind == "anti_simple":
+            val = T(2) * rho * w - prev
+        elif kind == "anti_o1":
+            val = T(2) * (w * rho * (T(1) + T(3) * dot(u, C[j]))) - prev
+        elif kind == "anti_o2":
+            uc = dot(u, C[j])
+            val = T(2) * (w * rho * (T(1) + T(3) * uc + uc * uc * T(0.5) * T(9)
+                                     - T(3) * norm2(u) * T(0.5))) - prev
+        else:
+            # std::pow(T, int) is evaluated in double, which carries the rest
+            # of the expression in double until the store into the T array.
+            uw = u + T(0.5) * (u - U[nb[sel]])
+            sq = np.float64(dot(uw, C[j])) ** 2
+            bracket = (1.0 + sq * 0.5 * 9.0) - np.float64(norm2(uw) * T(0.5) * T(3))
+            val = (np.float64(T(2) * rho * w) * bracket - np.float64(prev)).astype(lat.dtype)
+        R[j, xs] = val
+
+
+# ---------------------------------------------------------------------------
+# VTK DataArray bodies (test infrastructure for the device encoder).
+
+def vtk_crop(values, mesh, overlap, ncomp=1):
+    """Cells [overlap, n - overlap) per axis, x fastest, components interleaved
+    (util::CopyFromFieldArray, src/utils/util.h:439-540)."""
+    nx, ny, nz = mesh
+    v = np.asarray(values).reshape(nz, ny, nx, ncomp) if ncomp > 1 else \
+        np.asarray(values).reshape(nz, ny, nx)
+    o = overlap
+    return np.ascontiguousarray(v[o:nz - o, o:ny - o, o:nx - o]).reshape(-1)
+
+
+def vtk_body(data):
+    """Body of a binary base64 DataArray as Base64Encoder writes it
+    (src/io/base64.h; vti_writer.h:552-611): the data size in bytes as a
+    little-endian unsigned int, encoded on its own, then the data."""
+    import base64
+    raw = np.ascontiguousarray(data).tobytes()
+    size = np.array([len(raw) & 0xFFFFFFFF], dtype="<u4").tobytes()
+    return base64.b64encode(size).decode() + base64.b64encode(raw).decode()
+
+
+def vtk_arrays(path):
+    """{name: (type, ncomp, body)} of the DataArrays of a .vti file."""
+    import re
+    text = open(path, "rb").read().decode()
+    out = {}
+    for m in re.finditer(r'<DataArray type="(\w+)" Name="(\w+)" format="binary" '
+                         r'encoding="base64" NumberOfComponents="(\d+)">\n(.*?)\n</DataArray>',
+                         text, re.S):
+        out[m.group(2)] = (m.group(1), int(m.group(3)), m.group(4))
+    return out
+
+
+def vtk_decode(body, dtype):
+    """Values of a DataArray body (inverse of vtk_body)."""
+    import base64
+    size = np.frombuffer(base64.b64decode(body[:8]), dtype="<u4")[0]
+    data = base64.b64decode(body[8:])
+    assert len(data) == size
+    return np.frombuffer(data, dtype=dtype)

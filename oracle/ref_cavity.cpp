@@ -23,6 +23,18 @@
 //                  reference cell order; zero when unset)
 //   Ni        interior cells per axis (stored mesh is (Ni+2)^3, one void layer)
 //   RT        relaxation time tau (lattice units; dx = dt = 1 so u_lid is lattice)
+//   FLB_VTK_NAME=<name> (environment): after the main loop, the reference's
+//             vtmo writers write flag, rho, velocity, physRho, physVelocity
+//             into ./vtkoutput/vtidata/ (FLB_VTK_OVERLAP: overlap threshold).
+//   FLB_FIELDS_FILE (environment, single block): RHO (N values of T) and
+//             VELOCITY (3N, x y z per cell) replacing both fields after setup.
+//   FLB_POSTSTREAM_BB=<k> (environment): wall and lid cells collide with the
+//             bulk policy and the reference's post-stream managers
+//             BBLikeFixedBlockBdManager (boundary/boundary.h:86-140) run after
+//             every Stream(), as in examples/couette2d/couette2d.cpp:212-216:
+//             the lid (8) with bounceback::movingwall and the walls (4) with
+//             bounceback::normal (k=1), anti_simple (2), anti_O1 (3),
+//             anti_O2 (4) or anti_pressure (5) (bounce_back_boundary.h:167-256).
 //   blockfile optional BlockReader file (io/block_reader.h) for a multi-block run;
 //             NormalCommunicate() follows Stream() as in
 //             examples/cavity3d/cavity3d.cpp:220.
@@ -132,29 +144,99 @@ struct Runner {
     NSLattice.template getField<VELOCITY<T, LatSet::d>>().forEach(
       toplid, FlagFM, BBMovingWallFlag,
       [&](auto& field, std::size_t id) { field.SetField(id, LatU_Wall); });
+    // FLB_FIELDS_FILE (single block): N values of T for RHO, then 3N for
+    // VELOCITY (x y z per cell), replacing both fields on every cell.
+    if (const char* ff = std::getenv("FLB_FIELDS_FILE")) {
+      auto& blat = NSLattice.getBlockLat(0);
+      const std::size_t N = blat.getN();
+      std::vector<T> buf(4 * N);
+      std::ifstream in(ff, std::ios::binary);
+      in.read(reinterpret_cast<char*>(buf.data()), std::streamsize(buf.size() * sizeof(T)));
+      if (!in) {
+        std::fprintf(stderr, "FLB_FIELDS_FILE: short read\n");
+        std::exit(2);
+      }
+      auto& rhof = blat.template getField<RHO<T>>().getField(0);
+      auto& uf = blat.template getField<VELOCITY<T, LatSet::d>>().getField(0);
+      for (std::size_t id = 0; id < N; ++id) {
+        rhof[id] = buf[id];
+        for (int d = 0; d < 3; ++d) uf[id][d] = buf[N + 3 * id + d];
+      }
+    }
 
     using BulkTask = tmp::Key_TypePair<AABBFlag, BulkPolicy>;
     using BBTask = tmp::Key_TypePair<BouncebackFlag, collision::BounceBack<CELL>>;
     using BBMVTask = tmp::Key_TypePair<BBMovingWallFlag, collision::BounceBackMovingWall<CELL>>;
     using NSTask = TaskSelector<std::uint8_t, CELL, BulkTask, BBTask, BBMVTask>;
+    using AllBulkTask =
+      tmp::Key_TypePair<AABBFlag | BouncebackFlag | BBMovingWallFlag, BulkPolicy>;
+    using HWTask = TaskSelector<std::uint8_t, CELL, AllBulkTask>;
     using RhoUtask = tmp::Key_TypePair<AABBFlag, moment::rhoU<CELL, true>>;
     using RhoUTask = TaskSelector<std::uint8_t, CELL, RhoUtask>;
+    using LM = BlockLatticeManager<T, LatSet, FIELDS>;
+    using FM = BlockFieldManager<FLAG, T, 3>;
+    BBLikeFixedBlockBdManager<bounceback::normal<CELL>, LM, FM> NS_BB("NS_BB", NSLattice, FlagFM,
+                                                                      BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::anti_simple<CELL>, LM, FM> NS_ABB1(
+      "NS_ABB1", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::anti_O1<CELL>, LM, FM> NS_ABB2(
+      "NS_ABB2", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::anti_O2<CELL>, LM, FM> NS_ABB3(
+      "NS_ABB3", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::anti_pressure<CELL>, LM, FM> NS_ABB4(
+      "NS_ABB4", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
+    BBLikeFixedBlockBdManager<bounceback::movingwall<CELL>, LM, FM> NS_BBMW(
+      "NS_BBMW", NSLattice, FlagFM, BBMovingWallFlag, VoidFlag);
+    const char* hw = std::getenv("FLB_POSTSTREAM_BB");
+    const int wallkind = hw ? std::atoi(hw) : 0;
+    const bool poststream = wallkind >= 1 && wallkind <= 5;
 
     const bool multi = Geo.getBlockNum() > 1;
-    for (int i = 0; i < p.warmup; ++i) {
-      NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
-      NSLattice.Stream();
+    auto step = [&]() {
+      if (poststream) {
+        NSLattice.template ApplyCellDynamics<HWTask>(FlagFM);
+        NSLattice.Stream();
+        switch (wallkind) {
+          case 1: NS_BB.Apply(); break;
+          case 2: NS_ABB1.Apply(); break;
+          case 3: NS_ABB2.Apply(); break;
+          case 4: NS_ABB3.Apply(); break;
+          default: NS_ABB4.Apply(); break;
+        }
+        NS_BBMW.Apply();
+      } else {
+        NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
+        NSLattice.Stream();
+      }
       if (multi) NSLattice.NormalCommunicate();
-    }
+    };
+    for (int i = 0; i < p.warmup; ++i) step();
     Timer MainLoopTimer;
     MainLoopTimer.START_TIMER();
     while (MainLoopTimer() < p.steps) {
-      NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
-      NSLattice.Stream();
-      if (multi) NSLattice.NormalCommunicate();
+      step();
       ++MainLoopTimer;
     }
     MainLoopTimer.END_TIMER();
+    // FLB_VTK_NAME (environment): write the fields with the reference's vtmo
+    // writers into ./vtkoutput/vtidata/ of the working directory, before the
+    // rhoU output task (FLB_VTK_OVERLAP: the writers' overlap threshold).
+    if (const char* vn = std::getenv("FLB_VTK_NAME")) {
+      const char* vo = std::getenv("FLB_VTK_OVERLAP");
+      const int overlapth = vo ? std::atoi(vo) : -1;
+      vtmo::ScalarWriter FlagWriter("flag", FlagFM);
+      vtmo::ScalarWriter RhoWriter("rho", NSLattice.template getField<RHO<T>>());
+      vtmo::VectorWriter VecWriter("velocity", NSLattice.template getField<VELOCITY<T, LatSet::d>>());
+      vtmo::PhysScalarWriter PhysRhoWriter(
+        "physRho", NSLattice.template getField<RHO<T>>(),
+        std::bind(&BaseConverter<T>::getPhysRho, &BaseConv, std::placeholders::_1));
+      vtmo::PhysVectorWriter PhysVecWriter(
+        "physVelocity", NSLattice.template getField<VELOCITY<T, LatSet::d>>(),
+        std::bind(&BaseConverter<T>::template getPhysU<LatSet::d>, &BaseConv, std::placeholders::_1));
+      vtmo::vtmWriter<T, LatSet::d> Writer(vn, Geo, overlapth);
+      Writer.addWriterSet(FlagWriter, RhoWriter, VecWriter, PhysRhoWriter, PhysVecWriter);
+      Writer.WriteBinary(p.steps);
+    }
     const double ms = double(std::chrono::duration_cast<std::chrono::microseconds>(
                                MainLoopTimer.END - MainLoopTimer.START).count()) / 1000.0;
     const double cells = double(Geo.getTotalCellNum());

@@ -140,7 +140,8 @@ def test_set_launch_rejects_bad_shapes(gpu_ok):
         a.set_launch(8, 0, 1)     # FP32 builds 2 or 4 cells per thread
 
 
-@pytest.mark.parametrize("storage,vec", [("fp32", 2), ("fp16s", 2), ("fp64", 1)])
+@pytest.mark.parametrize("storage,vec", [("fp32", 2), ("fp32", 4), ("fp16s", 2), ("fp16s", 4),
+                                         ("fp64", 1), ("fp64", 2)])
 def test_every_vector_width_matches_oracle(gpu_ok, storage, vec):
     lat = F.cavity(21, tau=0.55, storage=storage)
     lat.set_launch(4, 0, vec)
@@ -149,3 +150,18 @@ def test_every_vector_width_matches_oracle(gpu_ok, storage, vec):
     ref.step(30)
     tol = {"fp32": 1e-5, "fp64": 1e-12, "fp16s": 2e-3}[storage]
     assert rel_maxnorm(lat.download_pops(), ref.pops) < tol
+
+
+@pytest.mark.parametrize("storage,widths", [("fp32", (2, 4)), ("fp16s", (2, 4)), ("fp64", (1, 2))])
+@pytest.mark.parametrize("ni", [21, 30])
+def test_vector_widths_are_bitwise_equal(gpu_ok, storage, widths, ni):
+    """Every cell's update is the same function of its 19 sources whatever the
+    cells per thread, so the vector widths agree bit for bit (ragged rows and
+    row ends included)."""
+    out = []
+    for v in widths:
+        lat = F.cavity(ni, tau=0.55, storage=storage)
+        lat.set_launch(2, 0, v)
+        lat.step(25)
+        out.append(lat.download_pops())
+    assert np.array_equal(out[0], out[1])

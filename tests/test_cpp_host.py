@@ -78,3 +78,31 @@ def test_host_example_runs_on_gpu_and_matches_oracle(gpu_ok, model):
     rrho, ru = ref.rhou_fields()
     assert rel_maxnorm(rho, rrho) < 1e-5
     assert rel_maxnorm(u, ru) < 1e-5
+
+
+@pytest.mark.gpu
+def test_host_example_halfway_bounce_back_managers(gpu_ok):
+    """BBLikeFixedBlockBdManager<bounceback::normal / movingwall> through the host
+    classes against the oracle's post-stream restatement."""
+    from freelb_b200 import build as B
+    from oracle import oracle as O
+    exe = B.build_examples()
+    ni, tau, steps = 16, 0.6, 60
+    n = ni + 2
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "out.bin")
+        r = subprocess.run([exe, str(ni), str(tau), "0.1", str(steps), "halfway", out],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        data = np.fromfile(out, dtype=np.float64)
+    N = n ** 3
+    fl = O.cavity_flags(ni)
+    ref = O.Lattice(n, n, n, fl, tau=tau, dtype=np.float32, keys=(2 | 4 | 8,), ops=(O.OP_BULK,))
+    ref.u.reshape(-1, 3)[fl == 8, 0] = np.float32(0.1)
+    for _ in range(steps):
+        ref.step(1)
+        O.poststream_bb(ref, 4, 1, "normal")
+        O.poststream_bb(ref, 8, 1, "movingwall")
+    rrho, ru = ref.rhou_fields()
+    assert rel_maxnorm(data[:N], rrho) < 1e-5
+    assert rel_maxnorm(data[N:], ru) < 1e-5

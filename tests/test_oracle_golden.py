@@ -189,3 +189,39 @@ def test_finite_difference_gradient_of_reference_solver():
     g_ref = (j_ref(ap) - j_ref(am)) / (2 * h)
     g_orc = (j_orc(ap) - j_orc(am)) / (2 * h)
     assert abs(g_ref - g_orc) <= 1e-7 * abs(g_ref)
+
+
+WALL_KINDS = {1: "normal", 2: "anti_simple", 3: "anti_o1", 4: "anti_o2", 5: "anti_pressure"}
+
+
+def seeded_fields(n, seed=7):
+    """RHO near 1 and small VELOCITY on every cell, so that each kind's
+    dependence on the fields is exercised."""
+    rng = np.random.default_rng(seed)
+    return 1.0 + rng.uniform(-0.02, 0.02, n ** 3), rng.uniform(-0.03, 0.03, (n ** 3, 3))
+
+
+@pytest.mark.skipif(O.ref_binary(np.float64) is None, reason="reference harness not built here")
+@pytest.mark.parametrize("wallkind", sorted(WALL_KINDS))
+def test_poststream_bb_restatement_matches_reference_managers(wallkind):
+    """oracle.poststream_bb against the reference's own BBLikeFixedBlockBdManager
+    applied after Stream(): bounceback::movingwall on the lid and, on the walls,
+    bounceback::normal / anti_simple / anti_O1 / anti_O2 / anti_pressure, with
+    seeded RHO and VELOCITY fields.  The anti kinds feed the fields back into
+    the walls every step and amplify the last-bit differences of the reference
+    build's FMA contraction, so the run is kept short."""
+    ni, steps = 8, 8
+    n = ni + 2
+    rho, u = seeded_fields(n)
+    for dt, tol in ((np.float64, 1e-12), (np.float32, 1e-5)):
+        ref = O.run_reference("bgk", ni, 0.6, 0.1, steps, 0, dtype=dt, threads=2,
+                              fields=(rho, u), poststream=wallkind)
+        fl = O.cavity_flags(ni)
+        lat = O.Lattice(n, n, n, fl, tau=0.6, dtype=dt, keys=(2 | 4 | 8,), ops=(O.OP_BULK,))
+        lat.rho[:] = rho.astype(dt)
+        lat.u.reshape(-1, 3)[:] = u.astype(dt)
+        for _ in range(steps):
+            lat.step(1)
+            O.poststream_bb(lat, 4, 1, WALL_KINDS[wallkind])
+            O.poststream_bb(lat, 8, 1, "movingwall")
+        assert rel_maxnorm(lat.pops, ref["pops"]) < tol, (wallkind, dt)
