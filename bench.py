@@ -336,13 +336,16 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, 
     flags = F.cavity_flags(ni)
     fluid = np.flatnonzero(flags == 2)
     cells = np.random.default_rng(seed + 1).choice(fluid, size=fd_cells, replace=False)
-    errs = []
+    errs, fds = [], []
     for c in cells:
         ap, am = alpha.copy(), alpha.copy()
         ap[c] += h
         am[c] -= h
         fd = (J(ap) - J(am)) / (2 * h)
+        fds.append(fd)
         errs.append(abs(g_alpha[c] - fd) / abs(fd))
+    fds = np.array(fds)
+    norm_err = float(np.linalg.norm(g_alpha[cells] - fds) / np.linalg.norm(fds))
     fd_tau = (J(t=tau + h) - J(t=tau - h)) / (2 * h)
     fd_ulid = (J(ulid=0.1 + h) - J(ulid=0.1 - h)) / (2 * h)
     return {"config": f"{ni}^3, T={steps}, checkpoints every {every}, tau={tau:.4f}",
@@ -354,6 +357,7 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, 
             "fd_cells": int(fd_cells),
             "fd_rel_err_alpha_max": float(np.max(errs)),
             "fd_rel_err_alpha_median": float(np.median(errs)),
+            "fd_rel_err_alpha_normwise": norm_err,
             "fd_rel_err_alpha": [float(e) for e in errs],
             "fd_rel_err_tau": float(abs(g_tau - fd_tau) / abs(fd_tau)),
             "fd_rel_err_ulid": float(abs(g_ulid - fd_ulid) / abs(fd_ulid))}

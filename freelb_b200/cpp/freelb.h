@@ -683,6 +683,11 @@ class BlockLatticeManager {
   void CuDevStream() { Stream(); }
   // one device block: the halo exchange between blocks has nothing to do
   void NormalCommunicate() {}
+  void NormalCommunicate(std::int64_t) {}
+  void NormalFullCommunicate() {}
+  void NormalFullCommunicate(std::int64_t) {}
+  void NormalAllCommunicate() {}
+  void NormalAllCommunicate(std::int64_t) {}
   void Communicate() {}
 
   void EnableToleranceU() { tolerance_on_ = true; }

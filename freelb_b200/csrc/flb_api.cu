@@ -107,6 +107,8 @@ struct flb_lattice {
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
   int ctas_per_sm = 0;
+  int prefetch = 0;             // L2 prefetch distance in CTAs; -1: resident CTAs of the GPU
+  int prefetch_auto[9][5] = {};  // resident CTAs per (tile_y, cells per thread), 0 = unknown
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -193,6 +195,8 @@ void build_params(flb_lattice* h) {
   p.pitch = b0.L.pitch;
   p.plane = b0.L.plane;
   p.dstride = h->dstride;
+  for (int i = 0; i < Q; ++i)
+    p.row_off[i] = i * h->dstride - (long long)cy(i) * p.pitch - (long long)cz(i) * p.plane;
   p.ntasks = d.ntasks;
   for (int t = 0; t < d.ntasks; ++t) {
     p.keys[t] = d.task_keys[t];
@@ -370,7 +374,21 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
     const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
     const long long per_cta = 32LL * h->tile_y;
     const dim3 grid(unsigned((chunks + per_cta - 1) / per_cta));
-    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(h->sp);
+    StepParams sp = h->sp;
+    sp.prefetch_ahead = h->prefetch > 0 ? h->prefetch : 0;
+    if (h->prefetch < 0) {
+      int& n = h->prefetch_auto[h->tile_y][V];
+      if (n == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull<S, R, MODEL, V>,
+                                                          32 * h->tile_y, 0) != cudaSuccess ||
+            per_sm < 1)
+          per_sm = 1;
+        n = per_sm * h->sm_count;
+      }
+      sp.prefetch_ahead = n;
+    }
+    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(sp);
   } else {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));
@@ -919,6 +937,14 @@ int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_th
   h->tile_y = tile_y;
   h->ctas_per_sm = ctas_per_sm;
   h->vec = v;
+  return FLB_OK;
+}
+
+int flb_set_prefetch(flb_lattice* h, int ctas_ahead) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (ctas_ahead < -1) return fail(FLB_ERR_INVALID, "prefetch distance %d < -1", ctas_ahead);
+  if (ctas_ahead != h->prefetch) drop_graphs(h);
+  h->prefetch = ctas_ahead;
   return FLB_OK;
 }
 

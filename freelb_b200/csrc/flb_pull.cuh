@@ -283,34 +283,51 @@ __device__ __forceinline__ uint2 hsplice_next(uint2 v, uint2 w) {
 }
 
 // The V post-stream words of chunk x0 of row (y, z): the same loads and edge
-// rules as gather_chunk (SIGN = +1), without conversion.
+// rules as gather_chunk (SIGN = +1), without conversion.  row_off, when given,
+// holds i * dstride - cy_i * pitch - cz_i * plane for the block (the source
+// row of direction i relative to the cell's own row).
+//
+// Row ends of inner rows: the source of x = 0 in a direction with c_x = +1 is
+// x = nx-1 of the row before (y - c_y - 1), and that of x = nx-1 with
+// c_x = -1 is x = 0 of the row after (y - c_y + 1); with at most two non-zero
+// components per D3Q19 velocity the carry reaches z only when the y row wraps,
+// and then c_z = 0.
 template <int V>
 __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, long long dstride,
                                              const Geom& g, int x0, int y, int z,
+                                             const long long* __restrict__ row_off,
                                              typename HWord<V>::type (&h)[Q]) {
   using W = typename HWord<V>::type;
   const bool inner_row = y > 0 && z > 0 && y < g.ny - 1 && z < g.nz - 1;
   if (inner_row) {
+    const __half* row = arr + g.base + (long long)y * g.pitch + (long long)z * g.plane;
     const int xprev = x0 >= V ? x0 - V : x0;
     const int xnext = x0 + V < g.nx ? x0 + V : x0;
+    const __half* rowp[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const __half* rowp = arr + i * dstride + g.base + (long long)(y - cy(i)) * g.pitch +
-                           (long long)(z - cz(i)) * g.plane;
-      const W v = hload<V>(rowp + x0);
+      rowp[i] = row + (row_off ? row_off[i]
+                               : i * dstride - (long long)cy(i) * g.pitch -
+                                     (long long)cz(i) * g.plane);
+      const W v = hload<V>(rowp[i] + x0);
       if (cx(i) == 0) {
         h[i] = v;
       } else if (cx(i) > 0) {
-        h[i] = hsplice_prev(hload<V>(rowp + xprev), v);
+        h[i] = hsplice_prev(hload<V>(rowp[i] + xprev), v);
       } else {
-        h[i] = hsplice_next(v, hload<V>(rowp + xnext));
+        h[i] = hsplice_next(v, hload<V>(rowp[i] + xnext));
       }
     }
     if (x0 == 0) {
 #pragma unroll
       for (int i = 1; i < Q; ++i)
-        if (cx(i) > 0)
-          hset(h[i], 0, hscalar(arr + i * dstride + wrap_off(g, 0, y, z, -cx(i), -cy(i), -cz(i))));
+        if (cx(i) > 0) {
+          const long long off = y - cy(i) - 1 >= 0
+                                    ? (long long)(g.nx - 1) - g.pitch
+                                    : (long long)(g.nx - 1) + (long long)(g.ny - 1) * g.pitch -
+                                          g.plane;
+          hset(h[i], 0, hscalar(rowp[i] + off));
+        }
     }
     const int klast = g.nx - 1 - x0;
     if (klast >= 0 && klast < V) {
@@ -319,10 +336,12 @@ __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, lon
         if (k == klast) {
 #pragma unroll
           for (int i = 1; i < Q; ++i)
-            if (cx(i) < 0)
-              hset(h[i], k,
-                   hscalar(arr + i * dstride +
-                           wrap_off(g, g.nx - 1, y, z, -cx(i), -cy(i), -cz(i))));
+            if (cx(i) < 0) {
+              const long long off = y - cy(i) + 1 <= g.ny - 1
+                                        ? (long long)g.pitch
+                                        : g.plane - (long long)(g.ny - 1) * g.pitch;
+              hset(h[i], k, hscalar(rowp[i] + off));
+            }
         }
     }
   } else {
@@ -338,60 +357,83 @@ __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, lon
   }
 }
 
-// BGK on deviations (see above); H[] in and out in units of the stored value.
-__device__ __forceinline__ void bgk_deviation(float (&H)[Q], float omega, float rho0,
-                                              float scale, float inv_scale) {
-  float sp[Q], df[Q];  // pair sums / differences, index of the first of the pair
+// Packed FP32 pairs: the two cells of a 32-bit half2 part travel as one float2
+// through sm_100's two-wide FP32 instructions (one instruction per pair).
+__device__ __forceinline__ float2 p2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {  // a - b, one rounding
+  return __ffma2_rn(b, p2(-1.0f), a);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  return __ffma2_rn(a, b, c);
+}
+
+// BGK on deviations (see above) for two cells at once; H[] in and out in units
+// of the stored value.  Every operation is an explicit two-wide instruction, so
+// each cell's result is the same whichever cell shares its pair.
+__device__ __forceinline__ void bgk_deviation2(float2 (&H)[Q], float omega, float rho0,
+                                               float scale, float inv_scale) {
+  float2 sp[Q], df[Q];  // pair sums / differences, index of the first of the pair
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
-    sp[i] = H[i] + H[i + 1];
-    df[i] = H[i] - H[i + 1];
+    sp[i] = add2(H[i], H[i + 1]);
+    df[i] = sub2(H[i], H[i + 1]);
   }
-  const float sum = ((H[0] + sp[1]) + (sp[3] + sp[5])) + ((sp[7] + sp[9]) + (sp[11] + sp[13])) +
-                    ((sp[15] + sp[17]));
-  const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
-  const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
-  const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
-  const float delta = sum * inv_scale;
-  const float rho = rho0 + delta;
-  const float ir = __fdividef(inv_scale, rho);  // 1 / (S rho)
-  const float ux = mx * ir, uy = my * ir, uz = mz * ir;
-  const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-  const float c1 = 1.0f - omega;
-  const float W0 = omega * scale * (1.0f / 3.0f);
-  const float W1 = omega * scale * (1.0f / 18.0f);
-  const float W2 = omega * scale * (1.0f / 36.0f);
-  const float d0 = W0 * delta, d1 = W1 * delta, d2 = W2 * delta;
-  const float r0 = W0 * rho, r1 = W1 * rho, r2 = W2 * rho;
-  const float k1 = 3.0f * ux, k3 = 3.0f * uy, k5 = 3.0f * uz;
-  float k[Q];
+  const float2 sum = add2(add2(add2(add2(H[0], sp[1]), add2(sp[3], sp[5])),
+                               add2(add2(sp[7], sp[9]), add2(sp[11], sp[13]))),
+                          add2(sp[15], sp[17]));
+  const float2 mx = add2(add2(add2(df[1], df[7]), add2(df[9], df[13])), df[15]);
+  const float2 my = add2(add2(add2(df[3], df[7]), sub2(df[11], df[13])), df[17]);
+  const float2 mz = sub2(add2(add2(df[5], df[9]), sub2(df[11], df[15])), df[17]);
+  const float2 delta = mul2(sum, p2(inv_scale));
+  const float2 rho = add2(p2(rho0), delta);
+  // 1 / (S rho)
+  const float2 ir = make_float2(__fdividef(inv_scale, rho.x), __fdividef(inv_scale, rho.y));
+  const float2 ux = mul2(mx, ir), uy = mul2(my, ir), uz = mul2(mz, ir);
+  const float2 q = mul2(p2(-1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
+  const float2 c1 = p2(1.0f - omega);
+  const float2 W0 = p2(omega * scale * (1.0f / 3.0f));
+  const float2 W1 = p2(omega * scale * (1.0f / 18.0f));
+  const float2 W2 = p2(omega * scale * (1.0f / 36.0f));
+  const float2 d0 = mul2(W0, delta), d1 = mul2(W1, delta), d2 = mul2(W2, delta);
+  const float2 r0 = mul2(W0, rho), r1 = mul2(W1, rho), r2 = mul2(W2, rho);
+  const float2 k1 = mul2(p2(3.0f), ux), k3 = mul2(p2(3.0f), uy), k5 = mul2(p2(3.0f), uz);
+  float2 k[Q];
   k[1] = k1;
   k[3] = k3;
   k[5] = k5;
-  k[7] = k1 + k3;
-  k[9] = k1 + k5;
-  k[11] = k3 + k5;
-  k[13] = k1 - k3;
-  k[15] = k1 - k5;
-  k[17] = k3 - k5;
-  H[0] = fmaf(r0, q, fmaf(c1, H[0], d0));
+  k[7] = add2(k1, k3);
+  k[9] = add2(k1, k5);
+  k[11] = add2(k3, k5);
+  k[13] = sub2(k1, k3);
+  k[15] = sub2(k1, k5);
+  k[17] = sub2(k3, k5);
+  H[0] = fma2(r0, q, fma2(c1, H[0], d0));
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
-    const float dw = i < 7 ? d1 : d2;
-    const float rw = i < 7 ? r1 : r2;
-    const float e = fmaf(0.5f * k[i], k[i], q);
-    H[i] = fmaf(rw, e + k[i], fmaf(c1, H[i], dw));
-    H[i + 1] = fmaf(rw, e - k[i], fmaf(c1, H[i + 1], dw));
+    const float2 dw = i < 7 ? d1 : d2;
+    const float2 rw = i < 7 ? r1 : r2;
+    const float2 e = fma2(mul2(p2(0.5f), k[i]), k[i], q);
+    H[i] = fma2(rw, add2(e, k[i]), fma2(c1, H[i], dw));
+    H[i + 1] = fma2(rw, sub2(e, k[i]), fma2(c1, H[i + 1], dw));
   }
 }
 
+// One cell: bulk BGK through the pair form (both lanes the same cell), other
+// ops through the generic operator on f = w_i rho0 + H / S.
 template <int MODEL>
 __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, float (&H)[Q],
                                                   long long cell, float omega) {
   if (op == OP_NONE) return;
   if constexpr (MODEL == MODEL_BGK) {
     if (op == OP_BULK) {
-      bgk_deviation(H, omega, p.rho0, p.scale, p.inv_scale);
+      float2 H2[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H2[i] = p2(H[i]);
+      bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H[i] = H2[i].x;
       return;
     }
   }
@@ -406,12 +448,13 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
 // One FP16S chunk, cells processed in pairs (the two halves of a 32-bit part).
 template <int MODEL, int V>
 __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom& g, float omega,
-                                                int x0, int y, int z) {
+                                                int x0, int y, int z,
+                                                const long long* row_off) {
   using W = typename HWord<V>::type;
   const __half* __restrict__ src = static_cast<const __half*>(p.src);
   __half* __restrict__ dst = static_cast<__half*>(p.dst);
   W h[Q];
-  gather_words<V>(src, p.dstride, g, x0, y, z, h);
+  gather_words<V>(src, p.dstride, g, x0, y, z, row_off, h);
   const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
   uint8_t fl[V];
   load_flags<V>(p.flags + cell0, fl);
@@ -419,6 +462,21 @@ __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom&
   for (int k = 0; k < V; k += 2) {
     const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
     if (opa == OP_NONE && opb == OP_NONE) continue;
+    if (MODEL == MODEL_BGK && opa == OP_BULK && opb == OP_BULK) {
+      float2 H2[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const unsigned q = hpart(h[i], k);
+        H2[i] = __half22float2(*reinterpret_cast<const __half2*>(&q));
+      }
+      bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const __half2 r = __float22half2_rn(H2[i]);
+        hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+      }
+      continue;
+    }
     float a[Q], b[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
@@ -443,9 +501,10 @@ __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom&
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
 template <typename S, typename R, int MODEL, int V>
 __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R omega, int lane,
-                                           int x0, int y, int z) {
+                                           int x0, int y, int z,
+                                           const long long* row_off = nullptr) {
   if constexpr (std::is_same<S, __half>::value && V >= 2) {
-    pull_chunk_half<MODEL, V>(p, g, omega, x0, y, z);
+    pull_chunk_half<MODEL, V>(p, g, omega, x0, y, z, row_off);
     return;
   }
   const S* __restrict__ src = static_cast<const S*>(p.src);
@@ -487,20 +546,66 @@ __device__ __forceinline__ bool chunk_coords(const Geom& g, long long q, int& x0
 // Single block: one thread per chunk; consecutive threads take consecutive
 // chunks, so a warp may span the end of one row and the start of the next and
 // only padding lanes idle.  Grid: ceil(chunks / blockDim.x) CTAs.
+// Minimum resident 256-thread CTAs per SM asked of the compiler: 2 caps the
+// FP32 and FP16S kernels at 128 registers (16 warps per SM), which measured
+// faster at 512^3 than the larger unbounded allocation; FP64 is left free.
+#ifndef FLB_PULL_MIN_CTAS
+#define FLB_PULL_MIN_CTAS 2
+#endif
+template <typename S>
+struct PullBounds {
+  static constexpr int min_ctas = std::is_same<S, double>::value ? 1 : FLB_PULL_MIN_CTAS;
+};
+
+// Bring the source rows of CTA t of the single-block grid into L2 (one bulk
+// prefetch per direction, issued by lanes 0..18 of the first warp): that CTA's
+// loads then wait on L2 rather than DRAM.  The range of direction i is the
+// CTA's cells shifted by -c_i (one cell of slack either side), clamped to the
+// direction's own array and widened to 16-byte bounds, which stay inside it
+// (arrays start 256-byte aligned and span a multiple of 64 elements).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+template <typename S, int V>
+__device__ __forceinline__ void prefetch_cta_sources(const StepParams& p, const Geom& g,
+                                                     long long t) {
+  const int i = threadIdx.x;
+  if (i >= Q) return;
+  const long long cpr = g.pitch / V;
+  const long long q0 = t * blockDim.x, q1 = q0 + blockDim.x - 1;
+  const long long c0 = (q0 / cpr) * g.pitch + (q0 % cpr) * V;
+  const long long c1 = (q1 / cpr) * g.pitch + (q1 % cpr) * V + (V - 1);
+  const long long shift = cx(i) + (long long)cy(i) * g.pitch + (long long)cz(i) * g.plane;
+  const long long total = g.plane * g.nz;
+  long long lo = c0 - shift - 1, hi = c1 - shift + 1;
+  if (lo < 0) lo = 0;
+  if (hi > total - 1) hi = total - 1;
+  if (lo > hi) return;
+  const char* base = static_cast<const char*>(p.src) + (long long)i * p.dstride * (long long)sizeof(S);
+  const unsigned long long a = reinterpret_cast<unsigned long long>(base + lo * (long long)sizeof(S)) & ~15ULL;
+  const unsigned long long e =
+      (reinterpret_cast<unsigned long long>(base + (hi + 1) * (long long)sizeof(S)) + 15ULL) & ~15ULL;
+  prefetch_l2(reinterpret_cast<const void*>(a), unsigned(e - a));
+}
+
 template <typename S, typename R, int MODEL, int V>
-__global__ void __launch_bounds__(256) k_pull(const StepParams p) {
+__global__ void __launch_bounds__(256, PullBounds<S>::min_ctas) k_pull(const StepParams p) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
+  if (p.prefetch_ahead > 0 && threadIdx.x < 32) {
+    const long long t = (long long)blockIdx.x + p.prefetch_ahead;
+    if (t < (long long)gridDim.x) prefetch_cta_sources<S, V>(p, g, t);
+  }
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int x0, y, z;
   if (!chunk_coords<V>(g, q, x0, y, z)) return;
-  pull_chunk<S, R, MODEL, V>(p, g, R(p.omega), 0, x0, y, z);
+  pull_chunk<S, R, MODEL, V>(p, g, R(p.omega), 0, x0, y, z, p.row_off);
 }
 
 // Many blocks: tiles of blockDim.x consecutive chunks, numbered block by block
 // (tile_start = first tile of the block); CTAs walk the tiles with a grid stride
 // (persistent) or take one tile each.
 template <typename S, typename R, int MODEL, int V>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, PullBounds<S>::min_ctas)
     k_pull_blocks(const StepParams p, const BlockEntry* __restrict__ blocks, int nblocks,
                   long long ntiles) {
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {

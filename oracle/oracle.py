@@ -193,7 +193,7 @@ def ref_binary(dtype=np.float32):
 
 def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float32,
                   blockfile=None, threads=None, outdir=None, alpha=None, fields=None,
-                  poststream=None):
+                  poststream=None, comm=None):
     """Run the reference's own CPU path; returns (dict of arrays, mlups)."""
     exe = ref_binary(dtype)
     if exe is None:
@@ -215,6 +215,8 @@ def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float3
         env["FLB_FIELDS_FILE"] = ffile
     if poststream is not None:  # wall kind 1..5 of the post-stream managers
         env["FLB_POSTSTREAM_BB"] = str(int(poststream))
+    if comm is not None:  # "full" / "all": NormalFullCommunicate / NormalAllCommunicate
+        env["FLB_COMM"] = comm
     args = [exe, model, str(ni), repr(float(tau)), repr(float(ulid)), str(steps), str(warmup),
             outdir, repr(float(cs))]
     if blockfile:
@@ -276,7 +278,10 @@ class MultiBlock:
     the cell lies beyond)."""
 
     def __init__(self, blocks, global_flags, n, model="bgk", tau=0.53, ulid=0.1, cs=0.1,
-                 mrt_rate=1.2, dtype=np.float32):
+                 mrt_rate=1.2, dtype=np.float32, full=False):
+        """full=True: normalFullCommunicate / normalAllCommunicate
+        (block_lattice.hh:1687-1720): all 19 populations of every overlap cell
+        owned by a neighbour (one overlap layer: the first layer is all)."""
         self.blocks = blocks
         self.lats = []
         gf = np.asarray(global_flags).reshape(n, n, n)
@@ -305,11 +310,13 @@ class MultiBlock:
             keep = own >= 0
             lx, ly, lz, gx, gy, gz, own = (a[keep] for a in (lx, ly, lz, gx, gy, gz, own))
             dst = lx + nx * (ly + ny * lz)
-            for i in range(1, 19):
+            for i in range(0 if full else 1, 19):
                 cxi, cyi, czi = C[i]
                 cross = np.zeros(lx.size, dtype=bool)
                 for l, m, c in ((lx, nx, cxi), (ly, ny, cyi), (lz, nz, czi)):
                     cross |= ((l == 0) & (c > 0)) | ((l == m - 1) & (c < 0))
+                if full:
+                    cross[:] = True
                 for o in np.unique(own[cross]):
                     sel = cross & (own == o)
                     nb = blocks[o]

@@ -36,7 +36,8 @@
 //             bounceback::normal (k=1), anti_simple (2), anti_O1 (3),
 //             anti_O2 (4) or anti_pressure (5) (bounce_back_boundary.h:167-256).
 //   blockfile optional BlockReader file (io/block_reader.h) for a multi-block run;
-//             NormalCommunicate() follows Stream() as in
+//             NormalCommunicate() (FLB_COMM=full / all: NormalFullCommunicate /
+//             NormalAllCommunicate) follows Stream() as in
 //             examples/cavity3d/cavity3d.cpp:220.
 //
 // Output (when outdir != "-"): meta.txt, flags.u8, pops.bin (19 x N, logical
@@ -187,6 +188,9 @@ struct Runner {
       "NS_ABB4", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
     BBLikeFixedBlockBdManager<bounceback::movingwall<CELL>, LM, FM> NS_BBMW(
       "NS_BBMW", NSLattice, FlagFM, BBMovingWallFlag, VoidFlag);
+    // FLB_COMM=full / all: NormalFullCommunicate / NormalAllCommunicate
+    const char* cm = std::getenv("FLB_COMM");
+    const int comm = cm ? (std::string(cm) == "full" ? 1 : (std::string(cm) == "all" ? 2 : 0)) : 0;
     const char* hw = std::getenv("FLB_POSTSTREAM_BB");
     const int wallkind = hw ? std::atoi(hw) : 0;
     const bool poststream = wallkind >= 1 && wallkind <= 5;
@@ -208,7 +212,11 @@ struct Runner {
         NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
         NSLattice.Stream();
       }
-      if (multi) NSLattice.NormalCommunicate();
+      if (multi) {
+        if (comm == 1) NSLattice.NormalFullCommunicate();
+        else if (comm == 2) NSLattice.NormalAllCommunicate();
+        else NSLattice.NormalCommunicate();
+      }
     };
     for (int i = 0; i < p.warmup; ++i) step();
     Timer MainLoopTimer;

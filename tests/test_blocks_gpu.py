@@ -165,3 +165,25 @@ def test_vector_widths_are_bitwise_equal(gpu_ok, storage, widths, ni):
         lat.step(25)
         out.append(lat.download_pops())
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_full_halo_matches_oracle(gpu_ok, storage, tol):
+    """flb_set_halo_mode(FULL): all 19 populations of every overlap cell from its
+    owner (NormalFullCommunicate / NormalAllCommunicate), against the oracle's
+    restatement (itself pinned to the reference's run)."""
+    ni, steps = 16, 20
+    blocks = G.uneven_blocks(ni, edges=(4, 6, 8), seed=3)
+    lat = gpu_blocks(ni, blocks, storage)
+    normal = lat.halo_count()
+    lat.set_halo_mode("full")
+    assert lat.halo_count() > normal
+    lat.step(steps)
+    dt = np.float64 if storage == "fp64" else np.float32
+    mb = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, dtype=dt, full=True)
+    mb.step(steps)
+    pops = np.concatenate([lat.download_pops(block=k) for k in range(len(blocks))])
+    want = np.concatenate([mb.lats[k].pops for k in range(len(blocks))])
+    assert rel_maxnorm(pops, want) < tol
+    lat.set_halo_mode("normal")
+    assert lat.halo_count() == normal

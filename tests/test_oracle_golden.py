@@ -125,6 +125,29 @@ def test_multiblock_restatement_matches_reference(name):
         assert np.array_equal(mb.lats[k].flags, g[f"flags_b{k}"])
 
 
+@pytest.mark.skipif(O.ref_binary(np.float64) is None, reason="reference harness not built here")
+@pytest.mark.parametrize("comm", ["full", "all"])
+def test_full_halo_restatement_matches_reference(comm, tmp_path):
+    """NormalFullCommunicate / NormalAllCommunicate (all populations of the
+    overlap cells), restated, against the reference's multi-block run."""
+    from freelb_b200 import geometry as G
+    ni, steps = 16, 20
+    blocks = G.uneven_blocks(ni, edges=(4, 6, 8), seed=3)
+    bf = str(tmp_path / "blocks.txt")
+    G.write_block_file(bf, blocks)
+    for dt, tol in ((np.float64, 1e-12), (np.float32, 1e-5)):
+        ref = O.run_reference("bgk", ni, 0.53, 0.1, steps, 0, dtype=dt, blockfile=bf, threads=2,
+                              comm=comm)
+        mb = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, dtype=dt, full=True)
+        mb.step(steps)
+        ours = np.concatenate([mb.lats[k].pops for k in range(len(blocks))])
+        want = np.concatenate([ref[f"pops_b{k}"] for k in range(len(blocks))])
+        assert rel_maxnorm(ours, want) < tol
+    normal = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, dtype=np.float32)
+    normal.step(steps)
+    assert not np.array_equal(np.concatenate([l.pops for l in normal.lats]), ours)
+
+
 def test_multiblock_equals_single_block_on_fluid_cells():
     from freelb_b200 import geometry as G
     blocks = G.uneven_blocks(16, edges=(4, 6, 8), seed=11)
