@@ -497,6 +497,9 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s",
                      "frac": ach32 / peak, "peak_source": peak_kind,
                      "traffic": (tr32 * cells if tr32 else None),
+                     "traffic_note": "DRAM bytes per cell of an ncu capture of the 202^3 cavity "
+                                     "(profiles/traffic.json) times the stored cells: the "
+                                     "traffic grows in proportion to the cells",
                      "algorithmic_bytes_per_cell": b32},
         "e2e": {"value": cells * args.steps * world / (e2e_ms / 1000.0) / 1e9, "unit": "GLUPs",
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,

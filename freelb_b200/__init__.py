@@ -223,11 +223,6 @@ class Lattice:
         C.call("flb_check_finite", self._h, ctypes.byref(v), _stream(stream))
         return int(v.value)
 
-    def set_prefetch(self, ctas_ahead):
-        """L2 prefetch distance of the single-block step kernel in CTAs (0 off,
-        -1 the GPU's resident CTAs)."""
-        C.call("flb_set_prefetch", self._h, int(ctas_ahead))
-
     def set_halo_mode(self, mode):
         """"normal" (NormalCommunicate) or "full" (NormalFullCommunicate /
         NormalAllCommunicate) halo exchange of a halo-mode block handle."""

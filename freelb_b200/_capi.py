@@ -107,7 +107,6 @@ SIGNATURES = {
     "flb_bb_apply": [_P, _P, _P],
     "flb_bb_destroy": [_P],
     "flb_set_halo_mode": [_P, _I],
-    "flb_set_prefetch": [_P, _I],
     "flb_vtk_field_base64": [_P, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
                              ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _P],
 }

@@ -107,8 +107,6 @@ struct flb_lattice {
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
   int ctas_per_sm = 0;
-  int prefetch = 0;             // L2 prefetch distance in CTAs; -1: resident CTAs of the GPU
-  int prefetch_auto[9][5] = {};  // resident CTAs per (tile_y, cells per thread), 0 = unknown
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -196,7 +194,7 @@ void build_params(flb_lattice* h) {
   p.plane = b0.L.plane;
   p.dstride = h->dstride;
   for (int i = 0; i < Q; ++i)
-    p.row_off[i] = i * h->dstride - (long long)cy(i) * p.pitch - (long long)cz(i) * p.plane;
+    p.row_off[i] = i * h->dstride - ((long long)cy(i) + (long long)cz(i) * p.ny) * p.pitch;
   p.ntasks = d.ntasks;
   for (int t = 0; t < d.ntasks; ++t) {
     p.keys[t] = d.task_keys[t];
@@ -374,21 +372,7 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
     const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
     const long long per_cta = 32LL * h->tile_y;
     const dim3 grid(unsigned((chunks + per_cta - 1) / per_cta));
-    StepParams sp = h->sp;
-    sp.prefetch_ahead = h->prefetch > 0 ? h->prefetch : 0;
-    if (h->prefetch < 0) {
-      int& n = h->prefetch_auto[h->tile_y][V];
-      if (n == 0) {
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pull<S, R, MODEL, V>,
-                                                          32 * h->tile_y, 0) != cudaSuccess ||
-            per_sm < 1)
-          per_sm = 1;
-        n = per_sm * h->sm_count;
-      }
-      sp.prefetch_ahead = n;
-    }
-    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(sp);
+    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(h->sp);
   } else {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));
@@ -638,6 +622,7 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
       (e = cudaMalloc(&h->rho, ds * h->real_bytes)) != cudaSuccess ||
       (e = cudaMalloc(&h->vel, 3 * ds * h->real_bytes)) != cudaSuccess ||
       (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess ||
+      (e = cudaMemset(h->acc, 0, 64)) != cudaSuccess ||
       (e = cudaMalloc((void**)&h->d_lut, 256)) != cudaSuccess)
     return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
   if (desc->model == FLB_MODEL_BRINKMAN) {
@@ -940,14 +925,6 @@ int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_th
   return FLB_OK;
 }
 
-int flb_set_prefetch(flb_lattice* h, int ctas_ahead) {
-  if (!h) return fail(FLB_ERR_INVALID, "null handle");
-  if (ctas_ahead < -1) return fail(FLB_ERR_INVALID, "prefetch distance %d < -1", ctas_ahead);
-  if (ctas_ahead != h->prefetch) drop_graphs(h);
-  h->prefetch = ctas_ahead;
-  return FLB_OK;
-}
-
 int flb_get_launch(const flb_lattice* h, int* tile_y, int* ctas_per_sm, int* cells_per_thread) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   if (tile_y) *tile_y = h->tile_y;
@@ -962,7 +939,8 @@ int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int
   if (trial_steps < 1) return fail(FLB_ERR_INVALID, "trial_steps %d < 1", trial_steps);
   cudaStream_t st = as_stream(stream);
   const int tys[] = {1, 2, 4, 8};
-  const int ctas[] = {0, 8, 16, 32};
+  const int ctas_list[] = {0, 8, 16, 32};
+  const int nctas = 4;
   const int vecs_d[] = {1, 2}, vecs_f[] = {2, 4};
   const int* vecs = h->desc.storage == FLB_STORAGE_FP64 ? vecs_d : vecs_f;
   const int ty0 = h->tile_y, c0 = h->ctas_per_sm, v0 = vec_width(h);
@@ -974,7 +952,8 @@ int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int
   int rc = FLB_OK;
   for (int vi = 0; vi < 2 && !rc; ++vi) {
     for (int ty : tys) {
-      for (int c : ctas) {
+      for (int ci = 0; ci < nctas; ++ci) {
+        const int c = ctas_list[ci];
         if ((rc = flb_set_launch(h, ty, c, vecs[vi]))) break;
         if ((rc = step_any(h, 1, st))) break;  // warm-up (block table upload, caches)
         cudaEventRecord(e0, st);

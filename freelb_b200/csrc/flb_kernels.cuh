@@ -28,7 +28,7 @@ struct StepParams {
   int nx, ny, nz, pitch;
   long long plane;    // pitch * ny
   long long dstride;  // elements between population arrays (and field planes)
-  long long row_off[Q];  // block 0: i * dstride - cy_i * pitch - cz_i * plane
+  long long row_off[Q];  // block 0: i * dstride - (cy_i + cz_i ny) * pitch
   int ntasks;
   uint8_t keys[8];
   uint8_t ops[8];
@@ -39,7 +39,6 @@ struct StepParams {
   float shift[Q];     // FP16S: rho0 * w_i
   float scale, inv_scale;
   float rho0;         // FP16S: density of the shift
-  int prefetch_ahead; // single-block step: L2 prefetch for the CTA this many ahead (0: off)
 };
 
 // First task whose key shares a bit with the flag (src/utils/tmp.h:283-309),

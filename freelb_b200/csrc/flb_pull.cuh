@@ -105,25 +105,39 @@ __device__ __forceinline__ long long wrap_off(const Geom& g, int x, int y, int z
   return g.base + sx + (long long)sy * g.pitch + (long long)sz * g.plane;
 }
 
+// Linear rows.  Rows are numbered r = z * ny + y over the block and the padded
+// layout stores row r at r * pitch, so the carry of y into z in the reference's
+// periodic shift over the linear cell index (CyclicArray::rotate,
+// field.h:676-697) is the linear order itself: the source row of direction i
+// is r - c_y - c_z ny, and a source x outside [0, nx) is x + nx of the row
+// before or x - nx of the row after.  Only the wrap of the whole block needs a
+// rule; rows with r in [ny + 2, ny nz - ny - 3] never reach it for any
+// direction or row-end source ("interior rows", which include the y = 0 and
+// y = ny-1 rows of all planes but the first two and last two).
+__device__ __forceinline__ bool interior_row(const Geom& g, int y, int z) {
+  const long long r = (long long)z * g.ny + y;
+  return r >= g.ny + 2 && r <= (long long)g.ny * g.nz - g.ny - 3;
+}
+
 // Gather, for the V cells x0.. of row (y, z), population i from the cell
 // SIGN*c_i away *before* it: SIGN = +1 reads x - c_i (streaming pull),
 // SIGN = -1 reads x + c_i (the transpose of streaming).
 //
-// Inner rows: every direction is one aligned V-wide load of the source row at
+// Interior rows: every direction is one aligned V-wide load of the source row at
 // the lane's own chunk; the ten x-shifted directions add one aligned load of
 // the adjacent chunk (the neighbour lane's, an L1 hit for all but one lane per
 // warp) and splice the element crossing the chunk edge.  The adjacent-chunk
 // addresses are clamped into the row, so the 29 loads carry no branches and can
 // all be in flight together.  Cells x = 0 / x = nx-1 whose sources cross the
-// row end and whole outer rows (y or z on the block surface) then re-load
-// through the wrap rule.  Called for chunks with x0 < nx only.
+// row end then re-load through the wrap rule; the rows near the block's first
+// and last planes (not interior) take every source through it.  Called for
+// chunks with x0 < nx only.
 template <typename S, typename R, int V, int SIGN>
 __device__ __forceinline__ void gather_chunk(const S* __restrict__ arr, long long dstride,
                                              const Geom& g, const float* shift, float inv_scale,
                                              int x0, int y, int z, R (&vals)[Q][V]) {
-  const bool inner_row = y > 0 && z > 0 && y < g.ny - 1 && z < g.nz - 1;
   const bool active = true;
-  if (inner_row) {
+  if (interior_row(g, y, z)) {
     const int xl = x0;
     const int xprev = xl >= V ? xl - V : xl;
     const int xnext = xl + V < g.nx ? xl + V : xl;
@@ -176,7 +190,7 @@ __device__ __forceinline__ void gather_chunk(const S* __restrict__ arr, long lon
         }
     }
   } else if (active) {
-    // outer row: every source through the wrap rule
+    // rows near the first and last planes: every source through the wrap rule
 #pragma unroll
     for (int k = 0; k < V; ++k) {
       const int x = min(x0 + k, g.nx - 1);
@@ -287,7 +301,7 @@ __device__ __forceinline__ uint2 hsplice_next(uint2 v, uint2 w) {
 // holds i * dstride - cy_i * pitch - cz_i * plane for the block (the source
 // row of direction i relative to the cell's own row).
 //
-// Row ends of inner rows: the source of x = 0 in a direction with c_x = +1 is
+// Row ends of interior rows: the source of x = 0 in a direction with c_x = +1 is
 // x = nx-1 of the row before (y - c_y - 1), and that of x = nx-1 with
 // c_x = -1 is x = 0 of the row after (y - c_y + 1); with at most two non-zero
 // components per D3Q19 velocity the carry reaches z only when the y row wraps,
@@ -298,8 +312,7 @@ __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, lon
                                              const long long* __restrict__ row_off,
                                              typename HWord<V>::type (&h)[Q]) {
   using W = typename HWord<V>::type;
-  const bool inner_row = y > 0 && z > 0 && y < g.ny - 1 && z < g.nz - 1;
-  if (inner_row) {
+  if (interior_row(g, y, z)) {
     const __half* row = arr + g.base + (long long)y * g.pitch + (long long)z * g.plane;
     const int xprev = x0 >= V ? x0 - V : x0;
     const int xnext = x0 + V < g.nx ? x0 + V : x0;
@@ -447,15 +460,10 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
 
 // One FP16S chunk, cells processed in pairs (the two halves of a 32-bit part).
 template <int MODEL, int V>
-__device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom& g, float omega,
-                                                int x0, int y, int z,
-                                                const long long* row_off) {
-  using W = typename HWord<V>::type;
-  const __half* __restrict__ src = static_cast<const __half*>(p.src);
+__device__ __forceinline__ void collide_store_half(const StepParams& p, float omega,
+                                                   long long cell0,
+                                                   typename HWord<V>::type (&h)[Q]) {
   __half* __restrict__ dst = static_cast<__half*>(p.dst);
-  W h[Q];
-  gather_words<V>(src, p.dstride, g, x0, y, z, row_off, h);
-  const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
   uint8_t fl[V];
   load_flags<V>(p.flags + cell0, fl);
 #pragma unroll
@@ -496,6 +504,16 @@ __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom&
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
+}
+
+template <int MODEL, int V>
+__device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom& g, float omega,
+                                                int x0, int y, int z,
+                                                const long long* row_off) {
+  typename HWord<V>::type h[Q];
+  gather_words<V>(static_cast<const __half*>(p.src), p.dstride, g, x0, y, z, row_off, h);
+  collide_store_half<MODEL, V>(
+      p, omega, g.base + (long long)y * g.pitch + (long long)z * g.plane + x0, h);
 }
 
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
@@ -557,44 +575,9 @@ struct PullBounds {
   static constexpr int min_ctas = std::is_same<S, double>::value ? 1 : FLB_PULL_MIN_CTAS;
 };
 
-// Bring the source rows of CTA t of the single-block grid into L2 (one bulk
-// prefetch per direction, issued by lanes 0..18 of the first warp): that CTA's
-// loads then wait on L2 rather than DRAM.  The range of direction i is the
-// CTA's cells shifted by -c_i (one cell of slack either side), clamped to the
-// direction's own array and widened to 16-byte bounds, which stay inside it
-// (arrays start 256-byte aligned and span a multiple of 64 elements).
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-template <typename S, int V>
-__device__ __forceinline__ void prefetch_cta_sources(const StepParams& p, const Geom& g,
-                                                     long long t) {
-  const int i = threadIdx.x;
-  if (i >= Q) return;
-  const long long cpr = g.pitch / V;
-  const long long q0 = t * blockDim.x, q1 = q0 + blockDim.x - 1;
-  const long long c0 = (q0 / cpr) * g.pitch + (q0 % cpr) * V;
-  const long long c1 = (q1 / cpr) * g.pitch + (q1 % cpr) * V + (V - 1);
-  const long long shift = cx(i) + (long long)cy(i) * g.pitch + (long long)cz(i) * g.plane;
-  const long long total = g.plane * g.nz;
-  long long lo = c0 - shift - 1, hi = c1 - shift + 1;
-  if (lo < 0) lo = 0;
-  if (hi > total - 1) hi = total - 1;
-  if (lo > hi) return;
-  const char* base = static_cast<const char*>(p.src) + (long long)i * p.dstride * (long long)sizeof(S);
-  const unsigned long long a = reinterpret_cast<unsigned long long>(base + lo * (long long)sizeof(S)) & ~15ULL;
-  const unsigned long long e =
-      (reinterpret_cast<unsigned long long>(base + (hi + 1) * (long long)sizeof(S)) + 15ULL) & ~15ULL;
-  prefetch_l2(reinterpret_cast<const void*>(a), unsigned(e - a));
-}
-
 template <typename S, typename R, int MODEL, int V>
 __global__ void __launch_bounds__(256, PullBounds<S>::min_ctas) k_pull(const StepParams p) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
-  if (p.prefetch_ahead > 0 && threadIdx.x < 32) {
-    const long long t = (long long)blockIdx.x + p.prefetch_ahead;
-    if (t < (long long)gridDim.x) prefetch_cta_sources<S, V>(p, g, t);
-  }
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int x0, y, z;
   if (!chunk_coords<V>(g, q, x0, y, z)) return;

@@ -268,11 +268,6 @@ FLB_API int flb_download_field_block(flb_lattice* lat, int block, int field, voi
  * and FP16S, 1 or 2 for FP64; 0 = default 2 / 4 / 2).  Defaults: tile_y 4, no
  * persistent grid. */
 FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm, int cells_per_thread);
-/* L2 prefetch of the single-block step kernel: each CTA first asks L2 for the
- * source rows of the CTA `ctas_ahead` positions later in the grid (one bulk
- * prefetch per direction), so those loads are served from L2.  0: off;
- * -1: as many CTAs ahead as the GPU holds resident; n > 0: n CTAs ahead. */
-FLB_API int flb_set_prefetch(flb_lattice* lat, int ctas_ahead);
 FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm,
                            int* cells_per_thread);
 
