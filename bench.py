@@ -456,7 +456,7 @@ def run_ours(args, rank, world, local_rank):
                 "launch": lch, "achieved_gbs": ach, "frac": ach / measured_peaks()[0],
                 "algorithmic_bytes_per_cell": b, "tau": tau, "nonfinite": bad}
         extras["variants"] = variants
-        extras["accuracy"] = accuracy_block(F, 256, 2000)
+        extras["accuracy"] = accuracy_block(F, args.accuracy_ni, 2000)
         extras["blocks_256"] = blocks_block(F, torch, stream, 256, args.steps)
         extras["ensemble_128"] = ensemble_block(F, torch, stream, args.steps)
         extras["adjoint_128"] = adjoint_block(F, torch, stream)
@@ -530,6 +530,8 @@ def main():
     ap.add_argument("--launch", default=None,
                     help="tile_y,ctas_per_sm,cells_per_thread for the headline run instead of "
                          "the autotuner (profiling)")
+    ap.add_argument("--accuracy-ni", type=int, default=256,
+                    help="cavity size of the FP64-referenced velocity error report (256 or 512)")
     ap.add_argument("--quick", action="store_true",
                     help="headline and e2e only (no variants / accuracy / blocks / ensemble / "
                          "adjoint blocks)")

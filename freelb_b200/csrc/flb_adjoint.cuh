@@ -21,6 +21,12 @@
 //     b = sum_i mu_i (w dfeq_i/du + (1 - w/2) dG_i/du)
 //     dJ/dtau   += -w^2 sum_i mu_i (feq_i - f_i - G_i/2)
 //     dJ/dalpha += b . (-u / (2 (rho + alpha/2))) + (1 - w/2) sum_i mu_i dG_i/dalpha|_u
+//   bulk MRT: C = f - A (f - feq), A = M^-1 S M, which is symmetric for the
+//   orthogonal basis (M^-1 = M^T diag(1/|M_k|^2)), so with nu = A mu
+//     lambda_j = mu_j - nu_j + sum nu feq / rho + (c_j - u) . b / rho,
+//     b = sum_i nu_i dfeq_i/du,
+//     dJ/dtau += w^2 sum over shear moments k of (M_k.mu)(M_k.(f - feq)) / |M_k|^2
+//   (the shear rates are w = 1/tau).
 // with the state R_t recomputed from checkpoints (flb_api.cu drives it).
 #pragma once
 
@@ -36,11 +42,83 @@ struct AdjParams {
   double* gpart;        // per thread block: [2b] dJ/dtau, [2b+1] dJ/du_lid partial sums
 };
 
-// Transposed Jacobian of one cell.  f: R_t of the cell, mu in, lam out.
+// Transposed Jacobian of a bulk MRT cell (see above).  s: per-moment rate over
+// |M_k|^2 as the forward step uses it.
 template <typename R>
-__device__ __forceinline__ void cell_vjp(int op, const R* f, const R* mu, R* lam, R omega,
-                                         R alpha, R rho_w, double& gtau, double& gulid,
-                                         double& galpha) {
+__device__ __forceinline__ void mrt_vjp(const R* f, const R* mu, R* lam, R omega, const R* s,
+                                        double& gtau) {
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  feq2(feq, rho, ux, uy, uz);
+  R am[9], bm[9], an[9], bn[9];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    am[p] = mu[2 * p + 1] + mu[2 * p + 2];
+    bm[p] = mu[2 * p + 1] - mu[2 * p + 2];
+    const R n1 = f[2 * p + 1] - feq[2 * p + 1], n2 = f[2 * p + 2] - feq[2 * p + 2];
+    an[p] = n1 + n2;
+    bn[p] = n1 - n2;
+  }
+  // dJ/dtau over the shear moments
+  double gt = 0;
+#pragma unroll
+  for (int k = 0; k < Q; ++k)
+    if (mrt_shear(k))
+      gt += double(mrt_moment<R>(k, mu[0], am, bm)) *
+            double(mrt_moment<R>(k, f[0] - feq[0], an, bn)) / double(mrt_norm(k));
+  gtau += double(omega) * double(omega) * gt;
+  // nu = A mu, from the forward relaxation applied to zero
+  R nu[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) nu[i] = R(0);
+  mrt_relax<R>(nu, mu[0], am, bm, s);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) nu[i] = -nu[i];
+  // weighted moments of nu (as in the BGK transpose)
+  R sp[Q], dp[Q];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = nu[i] + nu[i + 1];
+    dp[i] = nu[i] - nu[i + 1];
+  }
+  const R w0 = R(1) / R(3), wa = R(1) / R(18), wd = R(1) / R(36);
+  const R M0 = w0 * nu[0] + wa * ((sp[1] + sp[3]) + sp[5]) +
+               wd * (((sp[7] + sp[9]) + (sp[11] + sp[13])) + (sp[15] + sp[17]));
+  const R M1x = wa * dp[1] + wd * ((dp[7] + dp[9]) + (dp[13] + dp[15]));
+  const R M1y = wa * dp[3] + wd * ((dp[7] + dp[11]) + (dp[17] - dp[13]));
+  const R M1z = wa * dp[5] + wd * ((dp[9] + dp[11]) - (dp[15] + dp[17]));
+  const R Pxx = wa * sp[1] + wd * ((sp[7] + sp[9]) + (sp[13] + sp[15]));
+  const R Pyy = wa * sp[3] + wd * ((sp[7] + sp[11]) + (sp[13] + sp[17]));
+  const R Pzz = wa * sp[5] + wd * ((sp[9] + sp[11]) + (sp[15] + sp[17]));
+  const R Pxy = wd * (sp[7] - sp[13]);
+  const R Pxz = wd * (sp[9] - sp[15]);
+  const R Pyz = wd * (sp[11] - sp[17]);
+  const R Pux = Pxx * ux + Pxy * uy + Pxz * uz;
+  const R Puy = Pxy * ux + Pyy * uy + Pyz * uz;
+  const R Puz = Pxz * ux + Pyz * uy + Pzz * uz;
+  const R u2 = ux * ux + uy * uy + uz * uz;
+  const R feq_sum = M0 * (R(1) - R(1.5) * u2) + R(3) * (M1x * ux + M1y * uy + M1z * uz) +
+                    R(4.5) * (ux * Pux + uy * Puy + uz * Puz);
+  // b / rho = 3 M1 + 9 P u - 3 M0 u
+  const R qx = R(3) * M1x + R(9) * Pux - R(3) * M0 * ux;
+  const R qy = R(3) * M1y + R(9) * Puy - R(3) * M0 * uy;
+  const R qz = R(3) * M1z + R(9) * Puz - R(3) * M0 * uz;
+  const R base = feq_sum - (qx * ux + qy * uy + qz * uz);
+#pragma unroll
+  for (int j = 0; j < Q; ++j) {
+    R cb = base;
+    if (cx(j) > 0) cb += qx; else if (cx(j) < 0) cb -= qx;
+    if (cy(j) > 0) cb += qy; else if (cy(j) < 0) cb -= qy;
+    if (cz(j) > 0) cb += qz; else if (cz(j) < 0) cb -= qz;
+    lam[j] = mu[j] - nu[j] + cb;
+  }
+}
+
+// Transposed Jacobian of one cell.  f: R_t of the cell, mu in, lam out.
+template <typename R, int MODEL>
+__device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f, const R* mu,
+                                         R* lam, R omega, R alpha, R rho_w, double& gtau,
+                                         double& gulid, double& galpha) {
   if (op == OP_BB || op == OP_MBB) {
     lam[0] = mu[0];
 #pragma unroll
@@ -60,6 +138,14 @@ __device__ __forceinline__ void cell_vjp(int op, const R* f, const R* mu, R* lam
   if (op != OP_BULK) {
 #pragma unroll
     for (int i = 0; i < Q; ++i) lam[i] = mu[i];
+    return;
+  }
+  if constexpr (MODEL == MODEL_MRT) {
+    R s[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k)
+      s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm(k))) : R(p.s_over_norm[k]);
+    mrt_vjp<R>(f, mu, lam, omega, s, gtau);
     return;
   }
   R rho, den, ux, uy, uz;
@@ -129,7 +215,7 @@ __device__ __forceinline__ void cell_vjp(int op, const R* f, const R* mu, R* lam
 }
 
 // One backward step over a single block: lam_out = J_C^T S^T lam_in.
-template <typename R, int V>
+template <typename R, int V, int MODEL>
 __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const AdjParams a) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,7 +249,7 @@ __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const 
         const int op = select_op(p, fl[k]);
         const R al = alpha ? alpha[cell0 + k] : R(0);
         const R rw = op == OP_MBB ? rho[cell0 + k] : R(1);
-        cell_vjp<R>(op, f, m, l, omega, al, rw, gtau, gulid, ga);
+        cell_vjp<R, MODEL>(p, op, f, m, l, omega, al, rw, gtau, gulid, ga);
         if (op == OP_BULK && alpha) a.galpha[cell0 + k] += ga;
       } else {
 #pragma unroll

@@ -1146,8 +1146,9 @@ static int adjoint_supported(flb_lattice* h) {
     return fail(FLB_ERR_UNSUPPORTED, "the adjoint runs on single-block handles");
   if (h->desc.storage == FLB_STORAGE_FP16S)
     return fail(FLB_ERR_UNSUPPORTED, "the adjoint is built for FP32 and FP64 storage");
-  if (h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_BRINKMAN)
-    return fail(FLB_ERR_UNSUPPORTED, "the adjoint covers BGK and BRINKMAN bulk models");
+  if (h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_BRINKMAN &&
+      h->desc.model != FLB_MODEL_MRT)
+    return fail(FLB_ERR_UNSUPPORTED, "the adjoint covers BGK, BRINKMAN and MRT bulk models");
   for (int t = 0; t < h->desc.ntasks; ++t)
     if (h->desc.task_ops[t] == FLB_OP_FIELD_BGK)
       return fail(FLB_ERR_UNSUPPORTED, "the adjoint does not cover FIELD_BGK cells");
@@ -1174,6 +1175,21 @@ int flb_adjoint_forward(flb_lattice* h, int nsteps, int every, double* J, void* 
   }
   h->adj_T = nsteps;
   h->adj_k = every;
+  // the backward sweep's buffers, allocated here so that it allocates nothing:
+  // lambda (two arrays), dJ/dalpha and the every - 1 recompute slots
+  for (auto& p : h->adj_lam)
+    if (!p) FLB_CUDA(cudaMalloc(&p, bytes));
+  if (!h->adj_galpha)
+    FLB_CUDA(cudaMalloc((void**)&h->adj_galpha, size_t(h->dstride) * sizeof(double)));
+  while ((int)h->adj_seg.size() < every - 1) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      flb_adjoint_release(h);
+      return fail(FLB_ERR_OOM, "recompute slot (%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    h->adj_seg.push_back(p);
+  }
   for (int t = 0; t < nsteps; ++t) {
     if (t % every == 0)
       FLB_CUDA(cudaMemcpyAsync(h->adj_ckpt[t / every], h->pops[h->cur], bytes,
@@ -1244,7 +1260,10 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
       a.lam_in = h->adj_lam[cur];
       a.lam_out = h->adj_lam[cur ^ 1];
       a.q = q[t - t0];
-      k_adjoint_step<R, V><<<grid, block, 0, st>>>(h->sp, a);
+      if (h->desc.model == FLB_MODEL_MRT)
+        k_adjoint_step<R, V, MODEL_MRT><<<grid, block, 0, st>>>(h->sp, a);
+      else
+        k_adjoint_step<R, V, MODEL_BGK><<<grid, block, 0, st>>>(h->sp, a);
       cur ^= 1;
     }
     FLB_CUDA(cudaGetLastError());

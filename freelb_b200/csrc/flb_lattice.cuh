@@ -299,20 +299,37 @@ __device__ __forceinline__ void smagorinsky_bgk(R* f, R rt_mol, R cs_coeff) {
 // c -> -c, so even moments see only f_i + f_opp and odd ones only f_i - f_opp;
 // all basis entries are compile-time constants (zeros and unit factors fold).
 // s[k] already holds the per-moment rate divided by |M_k|^2.
+// Moment k of x given as r0 = x_0, a_p = x_{2p+1} + x_{2p+2}, b_p = x_{2p+1} -
+// x_{2p+2}: even moments see only a, odd ones only b.
 template <typename R>
-__device__ __forceinline__ void mrt(R* f, const R* s_over_norm) {
-  R rho, ux, uy, uz, feq[Q];
-  rho_u(f, rho, ux, uy, uz);
-  feq2(feq, rho, ux, uy, uz);
-  R a[9], b[9];  // symmetric / antisymmetric non-equilibrium parts per pair
-  const R r0 = f[0] - feq[0];
+__device__ __forceinline__ R mrt_moment(int k, R r0, const R (&a)[9], const R (&b)[9]) {
+  R m = R(0);
+  if (mrt_even(k)) {
+    if (mrt_m(k, 0) != 0) m = R(mrt_m(k, 0)) * r0;
 #pragma unroll
-  for (int p = 0; p < 9; ++p) {
-    const R n1 = f[2 * p + 1] - feq[2 * p + 1];
-    const R n2 = f[2 * p + 2] - feq[2 * p + 2];
-    a[p] = n1 + n2;
-    b[p] = n1 - n2;
+    for (int p = 0; p < 9; ++p) {
+      const int c = mrt_m(k, 2 * p + 1);
+      if (c == 1) m += a[p];
+      else if (c == -1) m -= a[p];
+      else if (c != 0) m += R(c) * a[p];
+    }
+  } else {
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      const int c = mrt_m(k, 2 * p + 1);
+      if (c == 1) m += b[p];
+      else if (c == -1) m -= b[p];
+      else if (c != 0) m += R(c) * b[p];
+    }
   }
+  return m;
+}
+
+// The moment-space relaxation of the non-equilibrium part: r0 = n_0,
+// a_p = n_{2p+1} + n_{2p+2}, b_p = n_{2p+1} - n_{2p+2}; x_i -= sum_k M[k][i] mu_k.
+template <typename R>
+__device__ __forceinline__ void mrt_relax(R* f, R r0, const R (&a)[9], const R (&b)[9],
+                                          const R* s_over_norm) {
   R mu[Q];
 #pragma unroll
   for (int k = 0; k < Q; ++k) {
@@ -361,6 +378,23 @@ __device__ __forceinline__ void mrt(R* f, const R* s_over_norm) {
     f[2 * p + 1] -= e + o;
     f[2 * p + 2] -= e - o;
   }
+}
+
+template <typename R>
+__device__ __forceinline__ void mrt(R* f, const R* s_over_norm) {
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  feq2(feq, rho, ux, uy, uz);
+  R a[9], b[9];  // symmetric / antisymmetric non-equilibrium parts per pair
+  const R r0 = f[0] - feq[0];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) {
+    const R n1 = f[2 * p + 1] - feq[2 * p + 1];
+    const R n2 = f[2 * p + 2] - feq[2 * p + 2];
+    a[p] = n1 + n2;
+    b[p] = n1 - n2;
+  }
+  mrt_relax<R>(f, r0, a, b, s_over_norm);
 }
 
 }  // namespace flb

@@ -433,12 +433,110 @@ __device__ __forceinline__ void bgk_deviation2(float2 (&H)[Q], float omega, floa
   }
 }
 
-// One cell: bulk BGK through the pair form (both lanes the same cell), other
-// ops through the generic operator on f = w_i rho0 + H / S.
+// Equilibrium of one cell in stored units, E_i = S (feq_i - w_i rho0)
+// = S w_i (delta + rho g_i), and the non-equilibrium part N_i = H_i - E_i =
+// S (f_i - feq_i), both without forming f_i (the deviation form above).
+__device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, float scale,
+                                              float inv_scale, float& rho, float (&N)[Q]) {
+  float sp[Q], df[Q];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = H[i] + H[i + 1];
+    df[i] = H[i] - H[i + 1];
+  }
+  const float sum = ((H[0] + sp[1]) + (sp[3] + sp[5])) + ((sp[7] + sp[9]) + (sp[11] + sp[13])) +
+                    (sp[15] + sp[17]);
+  const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
+  const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
+  const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
+  const float delta = sum * inv_scale;
+  rho = rho0 + delta;
+  const float ir = __fdividef(inv_scale, rho);
+  const float ux = mx * ir, uy = my * ir, uz = mz * ir;
+  const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
+  const float k1 = 3.0f * ux, k3 = 3.0f * uy, k5 = 3.0f * uz;
+  float k[Q];
+  k[1] = k1;
+  k[3] = k3;
+  k[5] = k5;
+  k[7] = k1 + k3;
+  k[9] = k1 + k5;
+  k[11] = k3 + k5;
+  k[13] = k1 - k3;
+  k[15] = k1 - k5;
+  k[17] = k3 - k5;
+  const float s0 = scale * (1.0f / 3.0f), s1 = scale * (1.0f / 18.0f),
+              s2 = scale * (1.0f / 36.0f);
+  N[0] = H[0] - s0 * fmaf(rho, q, delta);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float sw = i < 7 ? s1 : s2;
+    const float e = fmaf(0.5f * k[i], k[i], q);
+    N[i] = H[i] - sw * fmaf(rho, e + k[i], delta);
+    N[i + 1] = H[i + 1] - sw * fmaf(rho, e - k[i], delta);
+  }
+}
+
+// MRT (collision::MRT_Feq_RhoU) on deviations: H <- H - M^-1 S M N.
+__device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q], float omega) {
+  float rho, N[Q];
+  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
+  float a[9], b[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    a[q] = N[2 * q + 1] + N[2 * q + 2];
+    b[q] = N[2 * q + 1] - N[2 * q + 2];
+  }
+  float s[Q];
+#pragma unroll
+  for (int k = 0; k < Q; ++k)
+    s[k] = mrt_shear(k) ? omega * (1.0f / float(mrt_norm(k))) : float(p.s_over_norm[k]);
+  mrt_relax<float>(H, N[0], a, b, s);
+}
+
+// Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
+// sum c c N / S, the effective rate from it, H <- H - omega_eff N.
+__device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q], float omega) {
+  float rho, N[Q];
+  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
+  const float is = p.inv_scale;
+  const float p0 = is * ((((N[1] + N[2]) + (N[7] + N[8])) + ((N[9] + N[10]) + (N[13] + N[14]))) +
+                         (N[15] + N[16]));
+  const float p1 = is * ((N[7] + N[8]) - (N[13] + N[14]));
+  const float p2 = is * ((N[9] + N[10]) - (N[15] + N[16]));
+  const float p3 = is * ((((N[3] + N[4]) + (N[7] + N[8])) + ((N[11] + N[12]) + (N[13] + N[14]))) +
+                         (N[17] + N[18]));
+  const float p4 = is * ((N[11] + N[12]) - (N[17] + N[18]));
+  const float p5 = is * ((((N[5] + N[6]) + (N[9] + N[10])) + ((N[11] + N[12]) + (N[15] + N[16]))) +
+                         (N[17] + N[18]));
+  const float nsq = p0 * p0 + p1 * p1 * 2.0f + p2 * p2 * 2.0f + p3 * p3 + p4 * p4 * 2.0f + p5 * p5;
+  const float rt_mol = 1.0f / omega;
+  const float coeff = float(p.cs_coeff) / rho;
+  const float rt_tur = 0.5f * (sqrtf(rt_mol * rt_mol + coeff * sqrtf(nsq)) - rt_mol);
+  const float eomega = 1.0f / (rt_mol + rt_tur);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) H[i] = fmaf(-eomega, N[i], H[i]);
+}
+
+// One cell: bulk BGK through the pair form (both lanes the same cell), bulk
+// MRT and LES on deviations, other ops through the generic operator on
+// f = w_i rho0 + H / S.
 template <int MODEL>
 __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, float (&H)[Q],
                                                   long long cell, float omega) {
   if (op == OP_NONE) return;
+  if constexpr (MODEL == MODEL_MRT) {
+    if (op == OP_BULK) {
+      mrt_deviation(p, H, omega);
+      return;
+    }
+  }
+  if constexpr (MODEL == MODEL_LES) {
+    if (op == OP_BULK) {
+      les_deviation(p, H, omega);
+      return;
+    }
+  }
   if constexpr (MODEL == MODEL_BGK) {
     if (op == OP_BULK) {
       float2 H2[Q];

@@ -290,14 +290,17 @@ FLB_API int flb_objective_u2(flb_lattice* lat, double* J, void* stream);
 
 /* Discrete adjoint of the step (no reference counterpart: the reference has no
  * differentiation).  Single-block handles, FP32 or FP64 storage, ops none /
- * bulk (BGK or BRINKMAN) / bounce-back / moving wall.
+ * bulk (BGK, BRINKMAN or MRT) / bounce-back / moving wall.
  * flb_adjoint_forward advances nsteps from the current state, keeping a copy of
  * the state every `checkpoint_every` steps, and returns J at the end.
  * flb_adjoint_backward returns dJ/dalpha (per cell, N doubles in reference
  * order; may be NULL), dJ/dtau and dJ/du_lid (x-velocity of the moving-wall
  * cells), accumulated in FP64; the states between checkpoints are recomputed.
- * The lattice keeps the forward end state.  flb_adjoint_release frees the
- * checkpoint and adjoint memory. */
+ * The lattice keeps the forward end state.  flb_adjoint_forward allocates all
+ * device memory of the pair (ceil(nsteps / checkpoint_every) checkpoints and
+ * checkpoint_every - 1 recompute slots of the population size, two adjoint
+ * arrays, the dJ/dalpha array), so flb_adjoint_backward allocates nothing;
+ * flb_adjoint_release frees it. */
 FLB_API int flb_adjoint_forward(flb_lattice* lat, int nsteps, int checkpoint_every, double* J,
                                 void* stream);
 FLB_API int flb_adjoint_backward(flb_lattice* lat, double* dJ_dalpha, double* dJ_dtau,

@@ -109,6 +109,31 @@ def test_adjoint_plain_bgk_tau_and_lid(gpu_ok):
     assert abs(g_ulid - fd_u) <= 1e-6 * abs(fd_u), (g_ulid, fd_u)
 
 
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-6), ("fp32", 2e-3)])
+def test_adjoint_mrt_tau_and_lid(gpu_ok, storage, tol):
+    """MRT (Gram-Schmidt D3Q19 basis, shear rates 1/tau, others 1.2): the
+    transposed collision Jacobian gives dJ/dtau and dJ/du_lid matching FP64
+    central differences of the MRT forward."""
+    ni, tau, ulid, steps = 10, 0.58, 0.08, 40
+    lat = F.cavity(ni, tau=tau, ulid=ulid, storage=storage, model="mrt")
+    J = lat.adjoint_forward(steps, 16)
+    g_alpha, g_tau, g_ulid = lat.adjoint_backward(alpha_grad=False)
+
+    def Jf(t, u):
+        m = F.cavity(ni, tau=t, ulid=u, storage="fp64", model="mrt")
+        m.step(steps)
+        return m.objective_u2()
+
+    assert abs(J - Jf(tau, ulid)) / J < (1e-12 if storage == "fp64" else 1e-4)
+    h = 1e-4
+    d1 = (Jf(tau + h, ulid) - Jf(tau - h, ulid)) / (2 * h)
+    d2 = (Jf(tau + h / 2, ulid) - Jf(tau - h / 2, ulid)) / h
+    fd_tau = (4 * d2 - d1) / 3
+    fd_u = (Jf(tau, ulid + h) - Jf(tau, ulid - h)) / (2 * h)
+    assert abs(g_tau - fd_tau) <= tol * abs(fd_tau), (g_tau, fd_tau)
+    assert abs(g_ulid - fd_u) <= tol * abs(fd_u), (g_ulid, fd_u)
+
+
 def test_adjoint_rejects_unsupported(gpu_ok):
     lat = F.cavity(8, storage="fp16s")
     with pytest.raises(F.FlbError):
