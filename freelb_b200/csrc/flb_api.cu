@@ -195,6 +195,11 @@ void build_params(flb_lattice* h) {
   p.dstride = h->dstride;
   for (int i = 0; i < Q; ++i)
     p.row_off[i] = i * h->dstride - ((long long)cy(i) + (long long)cz(i) * p.ny) * p.pitch;
+  p.idx32 = h->blocks.size() == 1 && (long long)Q * h->dstride < (1LL << 32) ? 1 : 0;
+  for (int i = 0; i < Q; ++i) {
+    p.row_off32[i] = p.idx32 ? unsigned(p.row_off[i]) : 0u;
+    p.dir_off32[i] = p.idx32 ? unsigned(i * h->dstride) : 0u;
+  }
   p.ntasks = d.ntasks;
   for (int t = 0; t < d.ntasks; ++t) {
     p.keys[t] = d.task_keys[t];
@@ -366,7 +371,9 @@ int with_types(flb_lattice* h, F&& f) {
 
 template <typename S, typename R, int MODEL, int V>
 void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
-  const bool single = h->mode < 0 && h->ctas_per_sm == 0;
+  // the single-block kernel addresses with 32-bit offsets; larger lattices
+  // take the tile-table kernel
+  const bool single = h->mode < 0 && h->ctas_per_sm == 0 && h->sp.idx32;
   if (single) {
     const HostBlock& b = h->blocks[0];
     const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;

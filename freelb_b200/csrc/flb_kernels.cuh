@@ -29,6 +29,10 @@ struct StepParams {
   long long plane;    // pitch * ny
   long long dstride;  // elements between population arrays (and field planes)
   long long row_off[Q];  // block 0: i * dstride - (cy_i + cz_i ny) * pitch
+  // 32-bit element offsets for single-block handles with 19 * dstride < 2^32
+  unsigned row_off32[Q];  // row_off as an unsigned 32-bit offset
+  unsigned dir_off32[Q];  // i * dstride
+  int idx32;              // the 32-bit offsets above are valid
   int ntasks;
   uint8_t keys[8];
   uint8_t ops[8];

@@ -306,6 +306,69 @@ __device__ __forceinline__ uint2 hsplice_next(uint2 v, uint2 w) {
 // c_x = -1 is x = 0 of the row after (y - c_y + 1); with at most two non-zero
 // components per D3Q19 velocity the carry reaches z only when the y row wraps,
 // and then c_z = 0.
+// Rows near the block's first and last planes: every source through the wrap rule.
+template <int V>
+__device__ __forceinline__ void gather_words_wrap(const __half* __restrict__ arr,
+                                                  long long dstride, const Geom& g, int x0,
+                                                  int y, int z, typename HWord<V>::type (&h)[Q]) {
+  using W = typename HWord<V>::type;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) h[i] = W{};
+#pragma unroll
+  for (int k = 0; k < V; ++k) {
+    const int x = min(x0 + k, g.nx - 1);
+#pragma unroll
+    for (int i = 0; i < Q; ++i)
+      hset(h[i], k, hscalar(arr + i * dstride + wrap_off(g, x, y, z, -cx(i), -cy(i), -cz(i))));
+  }
+}
+
+// 32-bit form for single-block handles (19 * dstride < 2^32): every source is
+// arr + (cell + row_off32[i]), one 32-bit add and one wide multiply-add per
+// direction, and the adjacent chunk is at a fixed +-V (no clamp: on interior
+// rows the chunk before / after the row lies in the neighbouring row or the
+// padding, inside the array, and row-end lanes replace that element anyway).
+template <int V>
+__device__ __forceinline__ void gather_words32(const __half* __restrict__ arr,
+                                               long long dstride, const Geom& g, int x0, int y,
+                                               int z, const unsigned* __restrict__ row_off32,
+                                               typename HWord<V>::type (&h)[Q]) {
+  using W = typename HWord<V>::type;
+  const unsigned cell = unsigned((long long)y * g.pitch + (long long)z * g.plane + x0);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const __half* own = arr + (cell + row_off32[i]);
+    const W v = hload<V>(own);
+    if (cx(i) == 0) {
+      h[i] = v;
+    } else if (cx(i) > 0) {
+      h[i] = hsplice_prev(hload<V>(own - V), v);
+    } else {
+      h[i] = hsplice_next(v, hload<V>(own + V));
+    }
+  }
+  if (x0 == 0) {
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+      if (cx(i) > 0)
+        hset(h[i], 0,
+             hscalar(arr + i * dstride + wrap_off(g, 0, y, z, -cx(i), -cy(i), -cz(i))));
+  }
+  const int klast = g.nx - 1 - x0;
+  if (klast >= 0 && klast < V) {
+#pragma unroll
+    for (int k = 0; k < V; ++k)
+      if (k == klast) {
+#pragma unroll
+        for (int i = 1; i < Q; ++i)
+          if (cx(i) < 0)
+            hset(h[i], k,
+                 hscalar(arr + i * dstride +
+                         wrap_off(g, g.nx - 1, y, z, -cx(i), -cy(i), -cz(i))));
+      }
+  }
+}
+
 template <int V>
 __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, long long dstride,
                                              const Geom& g, int x0, int y, int z,
@@ -358,15 +421,7 @@ __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, lon
         }
     }
   } else {
-#pragma unroll
-    for (int i = 0; i < Q; ++i) h[i] = W{};
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-      const int x = min(x0 + k, g.nx - 1);
-#pragma unroll
-      for (int i = 0; i < Q; ++i)
-        hset(h[i], k, hscalar(arr + i * dstride + wrap_off(g, x, y, z, -cx(i), -cy(i), -cz(i))));
-    }
+    gather_words_wrap<V>(arr, dstride, g, x0, y, z, h);
   }
 }
 
@@ -557,7 +612,7 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
 }
 
 // One FP16S chunk, cells processed in pairs (the two halves of a 32-bit part).
-template <int MODEL, int V>
+template <int MODEL, int V, bool IDX32 = false>
 __device__ __forceinline__ void collide_store_half(const StepParams& p, float omega,
                                                    long long cell0,
                                                    typename HWord<V>::type (&h)[Q]) {
@@ -600,8 +655,14 @@ __device__ __forceinline__ void collide_store_half(const StepParams& p, float om
       hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
     }
   }
+  if constexpr (IDX32) {
+    const unsigned c32 = unsigned(cell0);
 #pragma unroll
-  for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
+    for (int i = 0; i < Q; ++i) hstore<V>(dst + (p.dir_off32[i] + c32), h[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
+  }
 }
 
 template <int MODEL, int V>
@@ -609,9 +670,18 @@ __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom&
                                                 int x0, int y, int z,
                                                 const long long* row_off) {
   typename HWord<V>::type h[Q];
-  gather_words<V>(static_cast<const __half*>(p.src), p.dstride, g, x0, y, z, row_off, h);
-  collide_store_half<MODEL, V>(
-      p, omega, g.base + (long long)y * g.pitch + (long long)z * g.plane + x0, h);
+  const __half* src = static_cast<const __half*>(p.src);
+  const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
+  if (row_off) {  // single block, 32-bit offsets (the host checks p.idx32)
+    if (interior_row(g, y, z))
+      gather_words32<V>(src, p.dstride, g, x0, y, z, p.row_off32, h);
+    else
+      gather_words_wrap<V>(src, p.dstride, g, x0, y, z, h);
+    collide_store_half<MODEL, V, true>(p, omega, cell0, h);
+  } else {
+    gather_words<V>(src, p.dstride, g, x0, y, z, nullptr, h);
+    collide_store_half<MODEL, V>(p, omega, cell0, h);
+  }
 }
 
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
