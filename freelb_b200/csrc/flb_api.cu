@@ -5,7 +5,7 @@
 // fields, a 64-byte result area for reductions, the block table and halo
 // records, and, on first use, a staging buffer for host transfers and the
 // captured CUDA graphs.  Blocks are packed one after another inside every
-// direction array (each block padded to pitch = nx rounded up to 32 and to a
+// direction array (each block padded to a row pitch, see row_pitch, and to a
 // multiple of 64 elements).  The C++17 classes in freelb_b200/cpp/freelb.h and
 // the Python module call only these functions.
 #include <cuda_runtime.h>
@@ -102,8 +102,9 @@ struct flb_lattice {
   long long ntiles = 0;
   int table_tile_y = 0;
   int table_vec = 0;
-  HaloCopy* d_halo = nullptr;
+  HaloCopy* d_halo = nullptr;   // records, or uint2 (src, dst) pairs when halo32
   long long nhalo = 0;
+  bool halo32 = false;
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
   int ctas_per_sm = 0;
@@ -257,6 +258,9 @@ int upload_op_lut(flb_lattice* h) {
   return FLB_OK;
 }
 
+// Elements per stored row: nx rounded up to 16.
+int row_pitch(int nx) { return (nx + 15) / 16 * 16; }
+
 // Block table for the tile kernel (rebuilt when tile_y changes).
 int upload_block_table(flb_lattice* h) {
   if (h->d_blocks && h->table_tile_y == h->tile_y && h->table_vec == vec_width(h)) return FLB_OK;
@@ -351,7 +355,19 @@ int build_halo(flb_lattice* h) {
   if (h->d_halo) cudaFree(h->d_halo);
   h->d_halo = nullptr;
   h->nhalo = (long long)recs.size();
-  if (!recs.empty()) {
+  h->halo32 = (long long)Q * h->dstride < (1LL << 32);
+  if (recs.empty()) return FLB_OK;
+  if (h->halo32) {
+    std::vector<uint2> pairs(recs.size());
+    for (size_t k = 0; k < recs.size(); ++k)
+      pairs[k] = make_uint2(unsigned(recs[k].dir * h->dstride + recs[k].src),
+                            unsigned(recs[k].dir * h->dstride + recs[k].dst));
+    std::sort(pairs.begin(), pairs.end(),
+              [](const uint2& a, const uint2& b) { return a.y < b.y; });
+    FLB_CUDA(cudaMalloc((void**)&h->d_halo, pairs.size() * sizeof(uint2)));
+    FLB_CUDA(cudaMemcpy(h->d_halo, pairs.data(), pairs.size() * sizeof(uint2),
+                        cudaMemcpyHostToDevice));
+  } else {
     FLB_CUDA(cudaMalloc((void**)&h->d_halo, recs.size() * sizeof(HaloCopy)));
     FLB_CUDA(cudaMemcpy(h->d_halo, recs.data(), recs.size() * sizeof(HaloCopy),
                         cudaMemcpyHostToDevice));
@@ -398,9 +414,14 @@ void launch_one_step(flb_lattice* h, cudaStream_t st) {
     if (v == 2) launch_one_step_v<S, R, MODEL, 2>(h, st);
     else launch_one_step_v<S, R, MODEL, 4>(h, st);
   }
-  if (h->nhalo > 0)
-    k_halo_pull<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, h->nhalo,
-                                                      static_cast<S*>(h->sp.dst), h->dstride);
+  if (h->nhalo > 0) {
+    if (h->halo32)
+      k_halo_pull32<S><<<grid_1d(h->nhalo), 256, 0, st>>>(
+          reinterpret_cast<const uint2*>(h->d_halo), h->nhalo, static_cast<S*>(h->sp.dst));
+    else
+      k_halo_pull<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, h->nhalo,
+                                                        static_cast<S*>(h->sp.dst), h->dstride);
+  }
 }
 
 template <typename S, typename R>
@@ -610,7 +631,7 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
   h->real_bytes = desc->storage == FLB_STORAGE_FP64 ? 8 : 4;
   long long off = 0;
   for (HostBlock& b : blocks) {
-    b.L.pitch = (b.L.nx + 15) / 16 * 16;
+    b.L.pitch = row_pitch(b.L.nx);
     b.L.plane = (long long)b.L.pitch * b.L.ny;
     b.base = off;
     off += (b.padded() + 63) / 64 * 64;
@@ -815,7 +836,8 @@ int flb_memory_bytes(const flb_lattice* h, size_t* bytes) {
   const size_t ds = size_t(h->dstride);
   *bytes = 2 * size_t(Q) * ds * h->elem_bytes + ds + 4 * ds * h->real_bytes + 64 +
            h->stage_bytes + (h->uprev ? 3 * ds * sizeof(double) : 0) +
-           h->blocks.size() * sizeof(BlockEntry) + size_t(h->nhalo) * sizeof(HaloCopy);
+           h->blocks.size() * sizeof(BlockEntry) +
+           size_t(h->nhalo) * (h->halo32 ? sizeof(uint2) : sizeof(HaloCopy));
   return FLB_OK;
 }
 

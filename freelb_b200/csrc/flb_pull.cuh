@@ -347,24 +347,20 @@ __device__ __forceinline__ void gather_words32(const __half* __restrict__ arr,
       h[i] = hsplice_next(v, hload<V>(own + V));
     }
   }
-  if (x0 == 0) {
+  if (x0 == 0) {  // x = nx-1 of the row before the source row
 #pragma unroll
     for (int i = 1; i < Q; ++i)
-      if (cx(i) > 0)
-        hset(h[i], 0,
-             hscalar(arr + i * dstride + wrap_off(g, 0, y, z, -cx(i), -cy(i), -cz(i))));
+      if (cx(i) > 0) hset(h[i], 0, hscalar(arr + (cell + row_off32[i] - g.pitch + (g.nx - 1))));
   }
   const int klast = g.nx - 1 - x0;
-  if (klast >= 0 && klast < V) {
+  if (klast >= 0 && klast < V) {  // x = 0 of the row after the source row
 #pragma unroll
-    for (int k = 0; k < V; ++k)
-      if (k == klast) {
+    for (int i = 1; i < Q; ++i)
+      if (cx(i) < 0) {
+        const unsigned e = hscalar(arr + (cell + row_off32[i] + g.pitch - x0));
 #pragma unroll
-        for (int i = 1; i < Q; ++i)
-          if (cx(i) < 0)
-            hset(h[i], k,
-                 hscalar(arr + i * dstride +
-                         wrap_off(g, g.nx - 1, y, z, -cx(i), -cy(i), -cz(i))));
+        for (int k = 0; k < V; ++k)
+          if (k == klast) hset(h[i], k, e);
       }
   }
 }
@@ -394,30 +390,20 @@ __device__ __forceinline__ void gather_words(const __half* __restrict__ arr, lon
         h[i] = hsplice_next(v, hload<V>(rowp[i] + xnext));
       }
     }
-    if (x0 == 0) {
+    if (x0 == 0) {  // x = nx-1 of the row before the source row
 #pragma unroll
       for (int i = 1; i < Q; ++i)
-        if (cx(i) > 0) {
-          const long long off = y - cy(i) - 1 >= 0
-                                    ? (long long)(g.nx - 1) - g.pitch
-                                    : (long long)(g.nx - 1) + (long long)(g.ny - 1) * g.pitch -
-                                          g.plane;
-          hset(h[i], 0, hscalar(rowp[i] + off));
-        }
+        if (cx(i) > 0) hset(h[i], 0, hscalar(rowp[i] - g.pitch + (g.nx - 1)));
     }
     const int klast = g.nx - 1 - x0;
-    if (klast >= 0 && klast < V) {
+    if (klast >= 0 && klast < V) {  // x = 0 of the row after the source row
 #pragma unroll
-      for (int k = 0; k < V; ++k)
-        if (k == klast) {
+      for (int i = 1; i < Q; ++i)
+        if (cx(i) < 0) {
+          const unsigned e = hscalar(rowp[i] + g.pitch);
 #pragma unroll
-          for (int i = 1; i < Q; ++i)
-            if (cx(i) < 0) {
-              const long long off = y - cy(i) + 1 <= g.ny - 1
-                                        ? (long long)g.pitch
-                                        : g.plane - (long long)(g.ny - 1) * g.pitch;
-              hset(h[i], k, hscalar(rowp[i] + off));
-            }
+          for (int k = 0; k < V; ++k)
+            if (k == klast) hset(h[i], k, e);
         }
     }
   } else {
@@ -914,6 +900,18 @@ __global__ void k_halo_pull(const HaloCopy* __restrict__ recs, long long n, S* p
        r += (long long)gridDim.x * blockDim.x) {
     const HaloCopy h = recs[r];
     pops[h.dir * dstride + h.dst] = pops[h.dir * dstride + h.src];
+  }
+}
+
+// The same copies as (source, destination) element indices into the whole
+// population buffer, 8 bytes per record instead of 24, when 19 x dstride <
+// 2^32; records sorted by destination.
+template <typename S>
+__global__ void k_halo_pull32(const uint2* __restrict__ recs, long long n, S* pops) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    const uint2 h = __ldg(recs + r);
+    pops[h.y] = pops[h.x];
   }
 }
 
