@@ -136,7 +136,7 @@ def test_pops_roundtrip_and_layout(gpu_ok):
         else:
             assert np.array_equal(back, p)
         L = lat.layout()
-        assert L.pitch_x % 16 == 0 and L.pitch_x >= nx and L.dir_stride % 64 == 0
+        assert L.pitch_x % 4 == 0 and L.pitch_x >= nx and L.dir_stride % 64 == 0
         f = rng.integers(0, 255, N, dtype=np.uint8)
         lat.upload_flags(f)
         assert np.array_equal(lat.download_flags(), f)
