@@ -65,7 +65,7 @@ __device__ __forceinline__ void mrt_vjp(const R* f, const R* mu, R* lam, R omega
   for (int k = 0; k < Q; ++k)
     if (mrt_shear(k))
       gt += double(mrt_moment<R>(k, mu[0], am, bm)) *
-            double(mrt_moment<R>(k, f[0] - feq[0], an, bn)) / double(mrt_norm(k));
+            double(mrt_moment<R>(k, f[0] - feq[0], an, bn)) / double(mrt_norm_lit(k));
   gtau += double(omega) * double(omega) * gt;
   // nu = A mu, from the forward relaxation applied to zero
   R nu[Q];
@@ -144,7 +144,7 @@ __device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f
     R s[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k)
-      s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm(k))) : R(p.s_over_norm[k]);
+      s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm_lit(k))) : R(p.s_over_norm[k]);
     mrt_vjp<R>(f, mu, lam, omega, s, gtau);
     return;
   }

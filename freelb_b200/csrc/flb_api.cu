@@ -23,6 +23,7 @@
 #include "../../include/flb.h"
 #include "../../include/flb_vtk.h"
 #include "flb_adjoint.cuh"
+#include "flb_pipe.cuh"
 #include "flb_vtk.cuh"
 
 using namespace flb;
@@ -107,7 +108,8 @@ struct flb_lattice {
   bool halo32 = false;
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
-  int ctas_per_sm = 0;
+  int ctas_per_sm = 0;  // -1: the FP16S async-copy pipeline (k_pull_pipe)
+  int pipe_ctas = 0;    // resident k_pull_pipe CTAs per SM (0 = not yet queried)
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -394,8 +396,61 @@ int with_types(flb_lattice* h, F&& f) {
   }
 }
 
+// The async-copy pipeline covers single-block FP16S handles with 32-bit
+// offsets (BGK, MRT, LES) at 4 cells per thread.
+bool pipe_supported(const flb_lattice* h) {
+  return h->desc.storage == FLB_STORAGE_FP16S && h->mode < 0 && h->sp.idx32 &&
+         h->desc.model != FLB_MODEL_BRINKMAN;
+}
+
+// 16-byte copies need 16-byte aligned rows.
+bool pipe_wide(const flb_lattice* h) { return h->blocks[0].L.pitch % 8 == 0; }
+
+template <int MODEL, bool WIDE>
+int pipe_prepare_w(flb_lattice* h) {
+  const int bytes = pipe_smem_bytes();
+  FLB_CUDA(cudaFuncSetAttribute(k_pull_pipe<MODEL, WIDE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  FLB_CUDA(cudaFuncSetAttribute(k_pull_pipe<MODEL, WIDE>,
+                                cudaFuncAttributePreferredSharedMemoryCarveout,
+                                int(cudaSharedmemCarveoutMaxShared)));
+  int n = 0;
+  FLB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pull_pipe<MODEL, WIDE>,
+                                                         PIPE_WARPS * 32, size_t(bytes)));
+  if (n < 1) return fail(FLB_ERR_CUDA, "k_pull_pipe does not fit on an SM");
+  h->pipe_ctas = n;
+  return FLB_OK;
+}
+
+template <int MODEL>
+int pipe_prepare_t(flb_lattice* h) {
+  return pipe_wide(h) ? pipe_prepare_w<MODEL, true>(h) : pipe_prepare_w<MODEL, false>(h);
+}
+
+int pipe_prepare(flb_lattice* h) {
+  if (h->pipe_ctas > 0) return FLB_OK;
+  switch (h->desc.model) {
+    case FLB_MODEL_MRT: return pipe_prepare_t<MODEL_MRT>(h);
+    case FLB_MODEL_LES: return pipe_prepare_t<MODEL_LES>(h);
+    default: return pipe_prepare_t<MODEL_BGK>(h);
+  }
+}
+
 template <typename S, typename R, int MODEL, int V>
 void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
+  if constexpr (std::is_same<S, __half>::value && V == PIPE_V && MODEL != MODEL_BRINKMAN) {
+    if (h->ctas_per_sm < 0) {  // flb_set_launch admits -1 only where pipe_supported
+      const HostBlock& b = h->blocks[0];
+      const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
+      const long long ctas_needed = ((chunks + 31) / 32 + PIPE_WARPS - 1) / PIPE_WARPS;
+      const long long g = std::max(1LL, std::min(ctas_needed, (long long)h->pipe_ctas * h->sm_count));
+      if (pipe_wide(h))
+        k_pull_pipe<MODEL, true><<<unsigned(g), PIPE_WARPS * 32, pipe_smem_bytes(), st>>>(h->sp);
+      else
+        k_pull_pipe<MODEL, false><<<unsigned(g), PIPE_WARPS * 32, pipe_smem_bytes(), st>>>(h->sp);
+      return;
+    }
+  }
   // the single-block kernel addresses with 32-bit offsets; larger lattices
   // take the tile-table kernel
   const bool single = h->mode < 0 && h->ctas_per_sm == 0 && h->sp.idx32;
@@ -953,9 +1008,17 @@ int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_th
                 cells_per_thread);
   if (tile_y != 1 && tile_y != 2 && tile_y != 4 && tile_y != 8)
     return fail(FLB_ERR_INVALID, "tile_y %d not in {1,2,4,8}", tile_y);
-  if (ctas_per_sm < 0 || ctas_per_sm > 32)
-    return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [0, 32]", ctas_per_sm);
+  if (ctas_per_sm < -1 || ctas_per_sm > 32)
+    return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [-1, 32]", ctas_per_sm);
   const int v = cells_per_thread ? cells_per_thread : default_vec(h->desc.storage);
+  if (ctas_per_sm < 0) {
+    if (!pipe_supported(h))
+      return fail(FLB_ERR_UNSUPPORTED,
+                  "ctas_per_sm -1 (async-copy pipeline) needs a single-block FP16S handle");
+    if (v != PIPE_V)
+      return fail(FLB_ERR_INVALID, "ctas_per_sm -1 runs %d cells per thread", PIPE_V);
+    FLB_TRY(pipe_prepare(h));
+  }
   if (tile_y != h->tile_y || ctas_per_sm != h->ctas_per_sm || v != vec_width(h)) drop_graphs(h);
   h->tile_y = tile_y;
   h->ctas_per_sm = ctas_per_sm;
@@ -1009,6 +1072,27 @@ int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int
         }
       }
       if (rc) break;
+    }
+  }
+  if (!rc && pipe_supported(h)) {  // the async-copy pipeline (fixed shape)
+    rc = flb_set_launch(h, 4, -1, PIPE_V);
+    if (!rc) rc = step_any(h, 1, st);
+    if (!rc) {
+      cudaEventRecord(e0, st);
+      rc = step_any(h, trial_steps, st);
+      cudaEventRecord(e1, st);
+    }
+    if (!rc) {
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      taken += trial_steps + 1;
+      if (ms < best) {
+        best = ms;
+        best_ty = 4;
+        best_c = -1;
+        best_v = PIPE_V;
+      }
     }
   }
   cudaEventDestroy(e0);

@@ -54,6 +54,22 @@ __device__ __forceinline__ int select_op(const StepParams& p, uint8_t flag) {
 enum : int { OP_NONE = 0, OP_BULK = 1, OP_BB = 2, OP_MBB = 3, OP_FIELD_BGK = 4 };
 enum : int { MODEL_BGK = 0, MODEL_MRT = 1, MODEL_LES = 2, MODEL_BRINKMAN = 3 };
 
+// The ops every model shares: bounce-back, moving wall, field-velocity BGK.
+template <typename R>
+__device__ __forceinline__ void apply_wall_op(const StepParams& p, int op, R* f, long long cell,
+                                              R omega) {
+  if (op == OP_BB) {
+    bounce_back<R>(f);
+  } else if (op == OP_MBB || op == OP_FIELD_BGK) {
+    const R* rho = static_cast<const R*>(p.rho);
+    const R* vel = static_cast<const R*>(p.vel);
+    const R rw = rho[cell];
+    const R ux = vel[cell], uy = vel[cell + p.dstride], uz = vel[cell + 2 * p.dstride];
+    if (op == OP_MBB) moving_wall<R>(f, rw, ux, uy, uz);
+    else bgk_field<R>(f, omega, R(1) - omega, rw, ux, uy, uz);
+  }
+}
+
 template <typename R, int MODEL>
 __device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long long cell,
                                          R omega) {
@@ -68,18 +84,11 @@ __device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long
       R s[Q];
 #pragma unroll
       for (int k = 0; k < Q; ++k)
-        s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm(k))) : R(p.s_over_norm[k]);
+        s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm_lit(k))) : R(p.s_over_norm[k]);
       mrt<R>(f, s);
     }
-  } else if (op == OP_BB) {
-    bounce_back<R>(f);
-  } else if (op == OP_MBB || op == OP_FIELD_BGK) {
-    const R* rho = static_cast<const R*>(p.rho);
-    const R* vel = static_cast<const R*>(p.vel);
-    const R rw = rho[cell];
-    const R ux = vel[cell], uy = vel[cell + p.dstride], uz = vel[cell + 2 * p.dstride];
-    if (op == OP_MBB) moving_wall<R>(f, rw, ux, uy, uz);
-    else bgk_field<R>(f, omega, R(1) - omega, rw, ux, uy, uz);
+  } else {
+    apply_wall_op<R>(p, op, f, cell, omega);
   }
 }
 

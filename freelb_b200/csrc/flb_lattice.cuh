@@ -70,6 +70,24 @@ __host__ __device__ constexpr int mrt_norm(int k) {
   for (int i = 0; i < Q; ++i) s += mrt_m(k, i) * mrt_m(k, i);
   return s;
 }
+// |M_k|^2 as literals: device code with a run-time k reads no table (a loop
+// over the velocity tables would put them on the stack).
+__host__ __device__ constexpr int mrt_norm_lit(int k) {
+  return k == 0 ? 19 : k == 1 ? 2394 : k == 2 ? 252 : k == 4 || k == 6 || k == 8 ? 40
+       : k == 9 ? 36 : k == 10 ? 72 : k == 11 ? 12 : k == 12 ? 24
+       : k >= 13 && k <= 15 ? 4 : k >= 16 ? 8 : 10;
+}
+static_assert(mrt_norm_lit(0) == mrt_norm(0) && mrt_norm_lit(1) == mrt_norm(1) &&
+                  mrt_norm_lit(2) == mrt_norm(2) && mrt_norm_lit(3) == mrt_norm(3) &&
+                  mrt_norm_lit(4) == mrt_norm(4) && mrt_norm_lit(5) == mrt_norm(5) &&
+                  mrt_norm_lit(6) == mrt_norm(6) && mrt_norm_lit(7) == mrt_norm(7) &&
+                  mrt_norm_lit(8) == mrt_norm(8) && mrt_norm_lit(9) == mrt_norm(9) &&
+                  mrt_norm_lit(10) == mrt_norm(10) && mrt_norm_lit(11) == mrt_norm(11) &&
+                  mrt_norm_lit(12) == mrt_norm(12) && mrt_norm_lit(13) == mrt_norm(13) &&
+                  mrt_norm_lit(14) == mrt_norm(14) && mrt_norm_lit(15) == mrt_norm(15) &&
+                  mrt_norm_lit(16) == mrt_norm(16) && mrt_norm_lit(17) == mrt_norm(17) &&
+                  mrt_norm_lit(18) == mrt_norm(18),
+              "MRT row norms");
 // Moments that are even under c -> -c (depend on f_i + f_opp(i) only).
 __host__ __device__ constexpr bool mrt_even(int k) {
   return k == 0 || k == 1 || k == 2 || (k >= 9 && k <= 15);

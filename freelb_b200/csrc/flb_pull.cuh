@@ -476,7 +476,10 @@ __device__ __forceinline__ void bgk_deviation2(float2 (&H)[Q], float omega, floa
 
 // Equilibrium of one cell in stored units, E_i = S (feq_i - w_i rho0)
 // = S w_i (delta + rho g_i), and the non-equilibrium part N_i = H_i - E_i =
-// S (f_i - feq_i), both without forming f_i (the deviation form above).
+// S (f_i - feq_i), both without forming f_i (the deviation form above).  Every
+// product that meets an addition is either an explicit fmaf or rounded on its
+// own (__fmul_rn), so no contraction is left to the compiler and the result is
+// the same in every kernel this is inlined into.
 __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, float scale,
                                               float inv_scale, float& rho, float (&N)[Q]) {
   float sp[Q], df[Q];
@@ -490,12 +493,12 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
   const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
   const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
   const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
-  const float delta = sum * inv_scale;
+  const float delta = sum * inv_scale;  // exact: inv_scale is a power of two
   rho = rho0 + delta;
   const float ir = __fdividef(inv_scale, rho);
   const float ux = mx * ir, uy = my * ir, uz = mz * ir;
   const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-  const float k1 = 3.0f * ux, k3 = 3.0f * uy, k5 = 3.0f * uz;
+  const float k1 = __fmul_rn(3.0f, ux), k3 = __fmul_rn(3.0f, uy), k5 = __fmul_rn(3.0f, uz);
   float k[Q];
   k[1] = k1;
   k[3] = k3;
@@ -508,13 +511,13 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
   k[17] = k3 - k5;
   const float s0 = scale * (1.0f / 3.0f), s1 = scale * (1.0f / 18.0f),
               s2 = scale * (1.0f / 36.0f);
-  N[0] = H[0] - s0 * fmaf(rho, q, delta);
+  N[0] = fmaf(-s0, fmaf(rho, q, delta), H[0]);
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
     const float sw = i < 7 ? s1 : s2;
     const float e = fmaf(0.5f * k[i], k[i], q);
-    N[i] = H[i] - sw * fmaf(rho, e + k[i], delta);
-    N[i + 1] = H[i + 1] - sw * fmaf(rho, e - k[i], delta);
+    N[i] = fmaf(-sw, fmaf(rho, e + k[i], delta), H[i]);
+    N[i + 1] = fmaf(-sw, fmaf(rho, e - k[i], delta), H[i + 1]);
   }
 }
 
@@ -531,16 +534,17 @@ __device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q]
   float s[Q];
 #pragma unroll
   for (int k = 0; k < Q; ++k)
-    s[k] = mrt_shear(k) ? omega * (1.0f / float(mrt_norm(k))) : float(p.s_over_norm[k]);
+    s[k] = mrt_shear(k) ? omega * (1.0f / float(mrt_norm_lit(k))) : float(p.s_over_norm[k]);
   mrt_relax<float>(H, N[0], a, b, s);
 }
 
 // Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
-// sum c c N / S, the effective rate from it, H <- H - omega_eff N.
+// sum c c N / S, the effective rate from it, H <- H - omega_eff N.  Products
+// that meet additions are explicit, as in deviation_neq.
 __device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q], float omega) {
   float rho, N[Q];
   deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
-  const float is = p.inv_scale;
+  const float is = p.inv_scale;  // a power of two: the scaling is exact
   const float p0 = is * ((((N[1] + N[2]) + (N[7] + N[8])) + ((N[9] + N[10]) + (N[13] + N[14]))) +
                          (N[15] + N[16]));
   const float p1 = is * ((N[7] + N[8]) - (N[13] + N[14]));
@@ -550,10 +554,15 @@ __device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q]
   const float p4 = is * ((N[11] + N[12]) - (N[17] + N[18]));
   const float p5 = is * ((((N[5] + N[6]) + (N[9] + N[10])) + ((N[11] + N[12]) + (N[15] + N[16]))) +
                          (N[17] + N[18]));
-  const float nsq = p0 * p0 + p1 * p1 * 2.0f + p2 * p2 * 2.0f + p3 * p3 + p4 * p4 * 2.0f + p5 * p5;
+  float nsq = __fmul_rn(p0, p0);
+  nsq = fmaf(__fmul_rn(p1, p1), 2.0f, nsq);
+  nsq = fmaf(__fmul_rn(p2, p2), 2.0f, nsq);
+  nsq = fmaf(p3, p3, nsq);
+  nsq = fmaf(__fmul_rn(p4, p4), 2.0f, nsq);
+  nsq = fmaf(p5, p5, nsq);
   const float rt_mol = 1.0f / omega;
   const float coeff = float(p.cs_coeff) / rho;
-  const float rt_tur = 0.5f * (sqrtf(rt_mol * rt_mol + coeff * sqrtf(nsq)) - rt_mol);
+  const float rt_tur = __fmul_rn(0.5f, sqrtf(fmaf(rt_mol, rt_mol, coeff * sqrtf(nsq))) - rt_mol);
   const float eomega = 1.0f / (rt_mol + rt_tur);
 #pragma unroll
   for (int i = 0; i < Q; ++i) H[i] = fmaf(-eomega, N[i], H[i]);
@@ -597,14 +606,12 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
   for (int i = 0; i < Q; ++i) H[i] = fmaf(f[i], p.scale, -p.shift[i] * p.scale);
 }
 
-// One FP16S chunk, cells processed in pairs (the two halves of a 32-bit part).
-template <int MODEL, int V, bool IDX32 = false>
-__device__ __forceinline__ void collide_store_half(const StepParams& p, float omega,
-                                                   long long cell0,
-                                                   typename HWord<V>::type (&h)[Q]) {
-  __half* __restrict__ dst = static_cast<__half*>(p.dst);
-  uint8_t fl[V];
-  load_flags<V>(p.flags + cell0, fl);
+// Collide one FP16S chunk in place, cells processed in pairs (the two halves
+// of a 32-bit part); fl holds the V cells' flags.
+template <int MODEL, int V>
+__device__ __forceinline__ void collide_half(const StepParams& p, float omega, long long cell0,
+                                             const uint8_t (&fl)[V],
+                                             typename HWord<V>::type (&h)[Q]) {
 #pragma unroll
   for (int k = 0; k < V; k += 2) {
     const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
@@ -641,6 +648,17 @@ __device__ __forceinline__ void collide_store_half(const StepParams& p, float om
       hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
     }
   }
+}
+
+// One FP16S chunk: flags, collision, one V-wide store per direction.
+template <int MODEL, int V, bool IDX32 = false>
+__device__ __forceinline__ void collide_store_half(const StepParams& p, float omega,
+                                                   long long cell0,
+                                                   typename HWord<V>::type (&h)[Q]) {
+  __half* __restrict__ dst = static_cast<__half*>(p.dst);
+  uint8_t fl[V];
+  load_flags<V>(p.flags + cell0, fl);
+  collide_half<MODEL, V>(p, omega, cell0, fl, h);
   if constexpr (IDX32) {
     const unsigned c32 = unsigned(cell0);
 #pragma unroll

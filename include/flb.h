@@ -265,8 +265,12 @@ FLB_API int flb_download_field_block(flb_lattice* lat, int block, int field, voi
 /* Launch shape of the stream-collide kernel: tile_y warps (rows) per CTA
  * (1, 2, 4 or 8), ctas_per_sm CTAs per SM for a persistent grid over the tile
  * work table (0 = one CTA per tile), and cells_per_thread (2 or 4 for FP32
- * and FP16S, 1 or 2 for FP64; 0 = default 2 / 4 / 2).  Defaults: tile_y 4, no
- * persistent grid. */
+ * and FP16S, 1 or 2 for FP64; 0 = default 2 / 4 / 2).  ctas_per_sm = -1
+ * selects, for single-block FP16S handles, the async-copy pipeline: a
+ * persistent grid (as many 4-warp CTAs as fit per SM) whose warps copy the next
+ * tile's sources into shared memory while the current tile collides; it runs 4
+ * cells per thread and ignores tile_y (FLB_ERR_UNSUPPORTED elsewhere).
+ * Defaults: tile_y 4, no persistent grid. */
 FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm, int cells_per_thread);
 FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm,
                            int* cells_per_thread);
