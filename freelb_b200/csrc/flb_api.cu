@@ -203,6 +203,10 @@ void build_params(flb_lattice* h) {
     p.row_off32[i] = p.idx32 ? unsigned(p.row_off[i]) : 0u;
     p.dir_off32[i] = p.idx32 ? unsigned(i * h->dstride) : 0u;
   }
+  // chunks per row of the single-block FP16S step (4 cells per chunk, or 2:
+  // the division constants depend on the chunk width, set at launch)
+  p.cpr_m = 0;
+  p.cpr_s = 0;
   p.ntasks = d.ntasks;
   for (int t = 0; t < d.ntasks; ++t) {
     p.keys[t] = d.task_keys[t];
@@ -436,6 +440,36 @@ int pipe_prepare(flb_lattice* h) {
   }
 }
 
+// Round-up division constants for q / d, q < 2^31 (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, Thm 4.2):
+// s = ceil(log2 d), m = ceil(2^(31+s) / d) < 2^32, q / d = (q m >> 32) >> (s - 1).
+// d = 1 gives m = 0 (no division).
+void division_constants(unsigned d, unsigned& m, unsigned& s) {
+  if (d <= 1) {
+    m = 0;
+    s = 0;
+    return;
+  }
+  unsigned sh = 0;
+  while ((1ull << sh) < d) ++sh;
+  m = unsigned(((1ull << (31 + sh)) + d - 1) / d);
+  s = sh;
+}
+
+// Direction bases of the single-block FP16S step for the launch's src / dst.
+template <int V>
+StepParams half_step_params(const flb_lattice* h) {
+  StepParams p = h->sp;
+  const __half* src = static_cast<const __half*>(p.src);
+  __half* dst = static_cast<__half*>(p.dst);
+  for (int i = 0; i < Q; ++i) {
+    p.src_dir[i] = src + p.row_off[i];
+    p.dst_dir[i] = dst + i * p.dstride;
+  }
+  division_constants(unsigned(p.pitch / V), p.cpr_m, p.cpr_s);
+  return p;
+}
+
 template <typename S, typename R, int MODEL, int V>
 void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
   if constexpr (std::is_same<S, __half>::value && V == PIPE_V && MODEL != MODEL_BRINKMAN) {
@@ -459,7 +493,10 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
     const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
     const long long per_cta = 32LL * h->tile_y;
     const dim3 grid(unsigned((chunks + per_cta - 1) / per_cta));
-    k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(h->sp);
+    if constexpr (std::is_same<S, __half>::value && V >= 2)
+      k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(half_step_params<V>(h));
+    else
+      k_pull<S, R, MODEL, V><<<grid, dim3(32 * h->tile_y), 0, st>>>(h->sp);
   } else {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));

@@ -33,6 +33,16 @@ struct StepParams {
   unsigned row_off32[Q];  // row_off as an unsigned 32-bit offset
   unsigned dir_off32[Q];  // i * dstride
   int idx32;              // the 32-bit offsets above are valid
+  // Per-launch direction bases of the single-block FP16S step (set from
+  // src / dst at launch): the source row of direction i relative to a cell,
+  // src + row_off[i], and the destination array, dst + i * dstride, so each
+  // address is the base plus the cell's 32-bit index.
+  const void* src_dir[Q];
+  void* dst_dir[Q];
+  // chunk -> row: row = umulhi(q, cpr_m) >> (cpr_s - 1) for q < 2^31, the
+  // round-up division by an invariant integer (Granlund & Montgomery, PLDI
+  // 1994); cpr_m = 0 when there is one chunk per row.
+  unsigned cpr_m, cpr_s;
   int ntasks;
   uint8_t keys[8];
   uint8_t ops[8];

@@ -323,21 +323,19 @@ __device__ __forceinline__ void gather_words_wrap(const __half* __restrict__ arr
   }
 }
 
-// 32-bit form for single-block handles (19 * dstride < 2^32): every source is
-// arr + (cell + row_off32[i]), one 32-bit add and one wide multiply-add per
-// direction, and the adjacent chunk is at a fixed +-V (no clamp: on interior
-// rows the chunk before / after the row lies in the neighbouring row or the
-// padding, inside the array, and row-end lanes replace that element anyway).
+// Single-block handles (19 * dstride < 2^32), interior rows: the source word
+// of direction i is src_dir[i] + cell (one wide multiply-add on a
+// kernel-parameter base), the adjacent chunk at a fixed +-V (no clamp: the
+// chunk before / after the row lies in the neighbouring row or the padding,
+// inside the array, and row-end lanes replace that element anyway).
 template <int V>
-__device__ __forceinline__ void gather_words32(const __half* __restrict__ arr,
-                                               long long dstride, const Geom& g, int x0, int y,
-                                               int z, const unsigned* __restrict__ row_off32,
-                                               typename HWord<V>::type (&h)[Q]) {
+__device__ __forceinline__ void gather_words_dir(const StepParams& p, const Geom& g, int x0,
+                                                 unsigned cell,
+                                                 typename HWord<V>::type (&h)[Q]) {
   using W = typename HWord<V>::type;
-  const unsigned cell = unsigned((long long)y * g.pitch + (long long)z * g.plane + x0);
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    const __half* own = arr + (cell + row_off32[i]);
+    const __half* own = static_cast<const __half*>(p.src_dir[i]) + cell;
     const W v = hload<V>(own);
     if (cx(i) == 0) {
       h[i] = v;
@@ -348,19 +346,21 @@ __device__ __forceinline__ void gather_words32(const __half* __restrict__ arr,
     }
   }
   if (x0 == 0) {  // x = nx-1 of the row before the source row
+    const unsigned e = cell - unsigned(g.pitch) + unsigned(g.nx - 1);
 #pragma unroll
     for (int i = 1; i < Q; ++i)
-      if (cx(i) > 0) hset(h[i], 0, hscalar(arr + (cell + row_off32[i] - g.pitch + (g.nx - 1))));
+      if (cx(i) > 0) hset(h[i], 0, hscalar(static_cast<const __half*>(p.src_dir[i]) + e));
   }
   const int klast = g.nx - 1 - x0;
   if (klast >= 0 && klast < V) {  // x = 0 of the row after the source row
+    const unsigned e = cell + unsigned(g.pitch) - unsigned(x0);
 #pragma unroll
     for (int i = 1; i < Q; ++i)
       if (cx(i) < 0) {
-        const unsigned e = hscalar(arr + (cell + row_off32[i] + g.pitch - x0));
+        const unsigned w = hscalar(static_cast<const __half*>(p.src_dir[i]) + e);
 #pragma unroll
         for (int k = 0; k < V; ++k)
-          if (k == klast) hset(h[i], k, e);
+          if (k == klast) hset(h[i], k, w);
       }
   }
 }
@@ -651,7 +651,7 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
 }
 
 // One FP16S chunk: flags, collision, one V-wide store per direction.
-template <int MODEL, int V, bool IDX32 = false>
+template <int MODEL, int V>
 __device__ __forceinline__ void collide_store_half(const StepParams& p, float omega,
                                                    long long cell0,
                                                    typename HWord<V>::type (&h)[Q]) {
@@ -659,42 +659,46 @@ __device__ __forceinline__ void collide_store_half(const StepParams& p, float om
   uint8_t fl[V];
   load_flags<V>(p.flags + cell0, fl);
   collide_half<MODEL, V>(p, omega, cell0, fl, h);
-  if constexpr (IDX32) {
-    const unsigned c32 = unsigned(cell0);
 #pragma unroll
-    for (int i = 0; i < Q; ++i) hstore<V>(dst + (p.dir_off32[i] + c32), h[i]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
-  }
+  for (int i = 0; i < Q; ++i) hstore<V>(dst + i * p.dstride + cell0, h[i]);
 }
 
 template <int MODEL, int V>
 __device__ __forceinline__ void pull_chunk_half(const StepParams& p, const Geom& g, float omega,
-                                                int x0, int y, int z,
-                                                const long long* row_off) {
+                                                int x0, int y, int z) {
   typename HWord<V>::type h[Q];
   const __half* src = static_cast<const __half*>(p.src);
   const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
-  if (row_off) {  // single block, 32-bit offsets (the host checks p.idx32)
-    if (interior_row(g, y, z))
-      gather_words32<V>(src, p.dstride, g, x0, y, z, p.row_off32, h);
-    else
-      gather_words_wrap<V>(src, p.dstride, g, x0, y, z, h);
-    collide_store_half<MODEL, V, true>(p, omega, cell0, h);
+  gather_words<V>(src, p.dstride, g, x0, y, z, nullptr, h);
+  collide_store_half<MODEL, V>(p, omega, cell0, h);
+}
+
+// Single-block FP16S chunk (19 * dstride < 2^32): linear row `row`, first cell
+// `cell` = row * pitch + x0; sources and stores through the direction bases.
+template <int MODEL, int V>
+__device__ __forceinline__ void pull_chunk_half32(const StepParams& p, const Geom& g, float omega,
+                                                  int x0, unsigned row, unsigned cell) {
+  typename HWord<V>::type h[Q];
+  if (int(row) >= g.ny + 2 && int(row) <= g.ny * g.nz - g.ny - 3) {  // interior_row
+    gather_words_dir<V>(p, g, x0, cell, h);
   } else {
-    gather_words<V>(src, p.dstride, g, x0, y, z, nullptr, h);
-    collide_store_half<MODEL, V>(p, omega, cell0, h);
+    const unsigned z = row / unsigned(g.ny);
+    gather_words_wrap<V>(static_cast<const __half*>(p.src), p.dstride, g, x0,
+                         int(row - z * unsigned(g.ny)), int(z), h);
   }
+  uint8_t fl[V];
+  load_flags<V>(p.flags + cell, fl);
+  collide_half<MODEL, V>(p, omega, (long long)cell, fl, h);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) hstore<V>(static_cast<__half*>(p.dst_dir[i]) + cell, h[i]);
 }
 
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
 template <typename S, typename R, int MODEL, int V>
 __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R omega, int lane,
-                                           int x0, int y, int z,
-                                           const long long* row_off = nullptr) {
+                                           int x0, int y, int z) {
   if constexpr (std::is_same<S, __half>::value && V >= 2) {
-    pull_chunk_half<MODEL, V>(p, g, omega, x0, y, z, row_off);
+    pull_chunk_half<MODEL, V>(p, g, omega, x0, y, z);
     return;
   }
   const S* __restrict__ src = static_cast<const S*>(p.src);
@@ -750,10 +754,21 @@ struct PullBounds {
 template <typename S, typename R, int MODEL, int V>
 __global__ void __launch_bounds__(256, PullBounds<S>::min_ctas) k_pull(const StepParams p) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
+  if constexpr (std::is_same<S, __half>::value && V >= 2) {
+    // 32-bit chunk index (fewer than 2^31 chunks: 19 * dstride < 2^32)
+    const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned cpr = unsigned(p.pitch) / V;
+    if (q >= cpr * unsigned(p.ny) * unsigned(p.nz)) return;
+    const unsigned row = p.cpr_m ? __umulhi(q, p.cpr_m) >> (p.cpr_s - 1) : q;
+    const int x0 = int(q - row * cpr) * V;
+    if (x0 >= p.nx) return;
+    pull_chunk_half32<MODEL, V>(p, g, float(p.omega), x0, row, q * V);
+    return;
+  }
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int x0, y, z;
   if (!chunk_coords<V>(g, q, x0, y, z)) return;
-  pull_chunk<S, R, MODEL, V>(p, g, R(p.omega), 0, x0, y, z, p.row_off);
+  pull_chunk<S, R, MODEL, V>(p, g, R(p.omega), 0, x0, y, z);
 }
 
 // Many blocks: tiles of blockDim.x consecutive chunks, numbered block by block
