@@ -740,19 +740,22 @@ __device__ __forceinline__ bool chunk_coords(const Geom& g, long long q, int& x0
 // Single block: one thread per chunk; consecutive threads take consecutive
 // chunks, so a warp may span the end of one row and the start of the next and
 // only padding lanes idle.  Grid: ceil(chunks / blockDim.x) CTAs.
-// Minimum resident 256-thread CTAs per SM asked of the compiler: 2 caps the
-// FP32 and FP16S kernels at 128 registers (16 warps per SM), which measured
-// faster at 512^3 than the larger unbounded allocation; FP64 is left free.
-#ifndef FLB_PULL_MIN_CTAS
-#define FLB_PULL_MIN_CTAS 2
-#endif
-template <typename S>
+// Minimum resident 256-thread CTAs per SM asked of the compiler, i.e. the
+// register cap: 3 (85 registers, 24 warps per SM) for the FP32 kernels at 2
+// cells per thread and the FP16S MRT / LES kernels, 2 (128 registers) for FP16S
+// BGK (its two-wide pair code spills badly at 85) and FP32 at 4 cells per
+// thread; FP64 is left free.  Measured at 512^3 against the other caps.
+template <typename S, int MODEL, int V>
 struct PullBounds {
-  static constexpr int min_ctas = std::is_same<S, double>::value ? 1 : FLB_PULL_MIN_CTAS;
+  static constexpr int min_ctas =
+      std::is_same<S, double>::value                          ? 1
+      : std::is_same<S, __half>::value && MODEL == MODEL_BGK ? 2
+      : std::is_same<S, float>::value && V == 4               ? 2
+                                                              : 3;
 };
 
 template <typename S, typename R, int MODEL, int V>
-__global__ void __launch_bounds__(256, PullBounds<S>::min_ctas) k_pull(const StepParams p) {
+__global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas) k_pull(const StepParams p) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
   if constexpr (std::is_same<S, __half>::value && V >= 2) {
     // 32-bit chunk index (fewer than 2^31 chunks: 19 * dstride < 2^32)
@@ -775,7 +778,7 @@ __global__ void __launch_bounds__(256, PullBounds<S>::min_ctas) k_pull(const Ste
 // (tile_start = first tile of the block); CTAs walk the tiles with a grid stride
 // (persistent) or take one tile each.
 template <typename S, typename R, int MODEL, int V>
-__global__ void __launch_bounds__(256, PullBounds<S>::min_ctas)
+__global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas)
     k_pull_blocks(const StepParams p, const BlockEntry* __restrict__ blocks, int nblocks,
                   long long ntiles) {
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
