@@ -291,6 +291,49 @@ BB_KINDS = {"normal": C.BB_NORMAL, "movingwall": C.BB_MOVINGWALL,
             "anti_pressure": C.BB_ANTI_PRESSURE}
 
 
+# NbrDirection bits (src/parallel/communicator.h:37-52)
+NBR = {"XN": 1, "XP": 2, "YN": 4, "YP": 8, "ZN": 16, "ZP": 32}
+
+
+class PeriodicBoundaryManager:
+    """FixedPeriodicBoundaryManager on a single-block lattice
+    (src/boundary/periodic_boundary.h:136-321): Setup(box0, dir0, box1, dir1)
+    at construction, apply() after each step (the reference calls Apply()
+    between ApplyCellDynamics and Stream; the collision is part of the step
+    here).  Boxes are inclusive stored-cell ranges (x0, x1, y0, y1, z0, z1);
+    directions are NbrDirection names ("XN", ...) or FLB_NBR_* bit masks."""
+
+    def __init__(self, lattice, box0, dir0, box1, dir1, cell_flag):
+        def bits(d):
+            return d if isinstance(d, int) else NBR[d]
+        self.lattice = lattice
+        b0 = (ctypes.c_int * 6)(*[int(v) for v in box0])
+        b1 = (ctypes.c_int * 6)(*[int(v) for v in box1])
+        h = ctypes.c_void_p()
+        C.call("flb_periodic_create", lattice._h, b0, bits(dir0), b1, bits(dir1), int(cell_flag),
+               ctypes.byref(h))
+        self._h = h
+
+    def counts(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        C.call("flb_periodic_count", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def apply(self, stream=None):
+        C.call("flb_periodic_apply", self._h, self.lattice._h, _stream(stream))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            C.load().flb_periodic_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BounceBackManager:
     """Post-stream halfway bounce-back on a single-block lattice:
     BBLikeFixedBlockBdManager<bounceback::KIND<CELL>, ...> with KIND one of

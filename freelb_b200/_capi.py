@@ -106,6 +106,12 @@ SIGNATURES = {
     "flb_bb_count": [_P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
     "flb_bb_apply": [_P, _P, _P],
     "flb_bb_destroy": [_P],
+    "flb_periodic_create": [_P, ctypes.POINTER(_I), _I, ctypes.POINTER(_I), _I, ctypes.c_uint8,
+                            ctypes.POINTER(_P)],
+    "flb_periodic_count": [_P, ctypes.POINTER(ctypes.c_longlong),
+                           ctypes.POINTER(ctypes.c_longlong)],
+    "flb_periodic_apply": [_P, _P, _P],
+    "flb_periodic_destroy": [_P],
     "flb_set_halo_mode": [_P, _I],
     "flb_vtk_field_base64": [_P, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
                              ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _P],

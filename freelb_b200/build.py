@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-EXAMPLES = ("cavity3d_b200", "cavity3d_vtk")
+EXAMPLES = ("cavity3d_b200", "cavity3d_vtk", "periodic3d_b200")
 EXAMPLE_SRC = os.path.join(HERE, "cpp", "examples", "cavity3d_b200.cpp")
 EXAMPLE_BIN = os.path.join(HERE, "cpp", "_build", "cavity3d_b200")
 

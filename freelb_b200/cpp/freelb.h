@@ -677,9 +677,18 @@ class BlockLatticeManager {
       flbcpp::check(flb_set_tasks(h_, 0, nullptr, nullptr, FLB_MODEL_BGK), "flb_set_tasks");
     }
     flbcpp::check(flb_step(h_, 1, nullptr), "flb_step");
+    // periodic managers whose Apply() came between ApplyCellDynamics and this
+    // Stream(): their copies act on the post-collision populations, which the
+    // fused step has just produced
+    for (flb_periodic* per : periodic_)
+      flbcpp::check(flb_periodic_apply(per, h_, nullptr), "flb_periodic_apply");
+    periodic_.clear();
     pending_ = false;
     fields_stale_ = true;
   }
+  // FixedPeriodicBoundaryManager::Apply(): runs after the next collision
+  void arm_periodic(flb_periodic* per) { periodic_.push_back(per); }
+  const BlockGeometry3D<T>& getGeo() const { return geo_; }
   void CuDevStream() { Stream(); }
   // one device block: the halo exchange between blocks has nothing to do
   void NormalCommunicate() {}
@@ -758,6 +767,7 @@ class BlockLatticeManager {
   bool pending_ = false;
   bool fields_stale_ = false;
   bool tolerance_on_ = false;
+  std::vector<flb_periodic*> periodic_;
 };
 
 // ---------------------------------------------------------------------------
@@ -818,6 +828,79 @@ class BBLikeFixedBlockBdManager final : public AbstractBlockBoundary {
   std::string name_;
   LatticeManager& lat_;
   flb_bb* h_ = nullptr;
+};
+
+// NbrDirection (parallel/communicator.h:37-52)
+enum NbrDirection : std::uint8_t {
+  NONE = 0,
+  XN = FLB_NBR_XN,
+  XP = FLB_NBR_XP,
+  YN = FLB_NBR_YN,
+  YP = FLB_NBR_YP,
+  ZN = FLB_NBR_ZN,
+  ZP = FLB_NBR_ZP
+};
+
+// FixedPeriodicBoundaryManager (boundary/periodic_boundary.h:136-321).
+// Setup(box0, dir0, box1, dir1) turns the two AABBs into stored-cell ranges
+// the way BasicBlock::getLocIdxRange does (basic_geometry.hh:448-472:
+// round((min - block min) / h) .. round((max - block min) / h) - 1, block min
+// = the domain's minimum less the overlap layer) and builds the device copy
+// list (flb_periodic_create); Apply(), called between ApplyCellDynamics and
+// Stream as in examples/couette2d/couette2d.cpp:212-214, makes the next
+// Stream() copy the post-collision populations box1 -> box0 over
+// getCommPopDir(dir0) and box0 -> box1 over getCommPopDir(dir1).
+template <typename LatticeManager, typename FlagManager>
+class FixedPeriodicBoundaryManager {
+ public:
+  using T = typename LatticeManager::FloatType;
+  FixedPeriodicBoundaryManager(std::string name, LatticeManager& lat, FlagManager& flags,
+                               std::uint8_t cellflag, std::uint8_t voidflag = std::uint8_t(1))
+      : name_(std::move(name)), lat_(lat), flags_(flags), cellflag_(cellflag),
+        voidflag_(voidflag) {}
+  ~FixedPeriodicBoundaryManager() { flb_periodic_destroy(h_); }
+  FixedPeriodicBoundaryManager(const FixedPeriodicBoundaryManager&) = delete;
+  FixedPeriodicBoundaryManager& operator=(const FixedPeriodicBoundaryManager&) = delete;
+
+  void Setup(const AABB<T, 3>& box0, NbrDirection dir0, const AABB<T, 3>& box1,
+             NbrDirection dir1) {
+    lat_.sync(flags_);
+    int b0[6], b1[6];
+    range(box0, b0);
+    range(box1, b1);
+    flb_periodic_destroy(h_);
+    h_ = nullptr;
+    flbcpp::check(flb_periodic_create(lat_.handle(), b0, int(dir0), b1, int(dir1), cellflag_, &h_),
+                  "flb_periodic_create");
+  }
+  void Apply() {
+    if (h_) lat_.arm_periodic(h_);
+  }
+  void getinfo() const {
+    long long pairs = 0;
+    if (h_) flb_periodic_count(h_, &pairs, nullptr);
+    std::cout << std::setw(18) << std::left << name_ << std::setw(10) << std::left << pairs
+              << std::endl;
+  }
+
+ private:
+  void range(const AABB<T, 3>& box, int* out) const {
+    const auto& g = lat_.getGeo();
+    const T h = g.getVoxelSize();
+    const Vector<T, 3> lo = g.getMinCenter() - Vector<T, 3>(T(0.5) * h);
+    const int n[3] = {g.getNx(), g.getNy(), g.getNz()};
+    for (int a = 0; a < 3; ++a) {
+      const int i0 = int(std::round((box.getMin()[a] - lo[a]) / h));
+      const int i1 = int(std::round((box.getMax()[a] - lo[a]) / h)) - 1;
+      out[2 * a] = i0 < 0 ? 0 : i0;
+      out[2 * a + 1] = i1 > n[a] - 1 ? n[a] - 1 : i1;
+    }
+  }
+  std::string name_;
+  LatticeManager& lat_;
+  FlagManager& flags_;
+  std::uint8_t cellflag_, voidflag_;
+  flb_periodic* h_ = nullptr;
 };
 
 // BlockBoundaryManager (basic_boundary.h:331-348): applies its managers in order.

@@ -1,4 +1,5 @@
-// flb_boundary.cu -- post-stream halfway bounce-back managers on the device.
+// flb_boundary.cu -- post-stream halfway bounce-back managers and the fixed
+// periodic boundary manager on the device.
 //
 // The reference's BBLikeFixedBlockBdManager (src/boundary/boundary.h:86-140)
 // visits, after Stream(), every inner cell whose flag matches `cell_flag` and,
@@ -155,9 +156,181 @@ int launch(flb_bb* bb, flb_lattice* lat, cudaStream_t st) {
   return FLB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Fixed periodic boundary: population copies between two boxes.
+
+// getCommPopDir (parallel/communicator.h:74-150): the directions entering a
+// cell across each face named in `dir`, sorted.
+std::vector<int> comm_pop_dirs(int dir) {
+  std::vector<int> out;
+  for (int i = 0; i < Q; ++i) {
+    const bool xs = (dir & FLB_NBR_XN) ? cx(i) > 0 : ((dir & FLB_NBR_XP) ? cx(i) < 0 : false);
+    const bool ys = (dir & FLB_NBR_YN) ? cy(i) > 0 : ((dir & FLB_NBR_YP) ? cy(i) < 0 : false);
+    const bool zs = (dir & FLB_NBR_ZN) ? cz(i) > 0 : ((dir & FLB_NBR_ZP) ? cz(i) < 0 : false);
+    if (xs || ys || zs) out.push_back(i);
+  }
+  return out;
+}
+
+// Cells of an inclusive box clamped to the mesh, z, y, x order (getCellIdx);
+// false when the box misses the interior [1, n-2] of some axis.
+bool box_cells(const flb_layout& L, const int* b, std::vector<long long>& cells) {
+  const int n[3] = {L.nx, L.ny, L.nz};
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    if (b[2 * a] > n[a] - 2 || b[2 * a + 1] < 1 || b[2 * a] > b[2 * a + 1]) return false;
+    lo[a] = b[2 * a] < 0 ? 0 : b[2 * a];
+    hi[a] = b[2 * a + 1] > n[a] - 1 ? n[a] - 1 : b[2 * a + 1];
+  }
+  for (int z = lo[2]; z <= hi[2]; ++z)
+    for (int y = lo[1]; y <= hi[1]; ++y)
+      for (int x = lo[0]; x <= hi[0]; ++x)
+        cells.push_back(x + (long long)y * L.pitch_x + (long long)z * (long long)L.plane);
+  return true;
+}
+
+template <typename E>
+__global__ void k_gather(const long long* __restrict__ src, long long n, const E* pops, E* stage) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x)
+    stage[r] = pops[src[r]];
+}
+template <typename E>
+__global__ void k_scatter(const long long* __restrict__ dst, long long n, const E* stage, E* pops) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x)
+    pops[dst[r]] = stage[r];
+}
+
+template <typename E>
+int periodic_launch(flb_periodic* per, void* pops, cudaStream_t st);
+
+}  // namespace
+
+struct flb_periodic {
+  flb_layout layout{};
+  long long npairs = 0;
+  long long ncopies = 0;
+  long long* d_src = nullptr;  // element offset of each copy's source slot
+  long long* d_dst = nullptr;  // and of its destination slot
+  void* d_stage = nullptr;     // ncopies elements
+};
+
+namespace {
+template <typename E>
+int periodic_launch(flb_periodic* per, void* pops, cudaStream_t st) {
+  const long long n = per->ncopies;
+  const unsigned grid = unsigned(n / 256 + 1 < 4096 ? n / 256 + 1 : 4096);
+  k_gather<E><<<grid, 256, 0, st>>>(per->d_src, n, static_cast<const E*>(pops),
+                                    static_cast<E*>(per->d_stage));
+  k_scatter<E><<<grid, 256, 0, st>>>(per->d_dst, n, static_cast<const E*>(per->d_stage),
+                                     static_cast<E*>(pops));
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char m[160];
+    std::snprintf(m, sizeof m, "flb_periodic_apply: %s", cudaGetErrorString(e));
+    return report_error(FLB_ERR_CUDA, m);
+  }
+  return FLB_OK;
+}
 }  // namespace
 
 extern "C" {
+
+int flb_periodic_create(flb_lattice* lat, const int box0[6], int dir0, const int box1[6],
+                        int dir1, uint8_t cell_flag, flb_periodic** out) {
+  if (!lat || !box0 || !box1 || !out)
+    return report_error(FLB_ERR_INVALID, "flb_periodic_create: null argument");
+  *out = nullptr;
+  if (dir0 < 0 || dir0 > 63 || dir1 < 0 || dir1 > 63)
+    return report_error(FLB_ERR_INVALID, "flb_periodic_create: direction outside the FLB_NBR_* bits");
+  int nblocks = 0;
+  int rc = flb_block_count(lat, &nblocks);
+  if (rc) return rc;
+  if (nblocks != 1)
+    return report_error(FLB_ERR_UNSUPPORTED, "flb_periodic_create: single-block lattices only");
+  flb_layout L{};
+  if ((rc = flb_get_layout(lat, &L))) return rc;
+  const long long N = (long long)L.nx * L.ny * L.nz;
+  std::vector<uint8_t> flags(static_cast<size_t>(N));
+  if ((rc = flb_download_flags(lat, flags.data(), nullptr))) return rc;
+  bool any = false;  // NonLocalBoundary::Setup (basic_boundary.h:395-420): the block's BdCells
+  for (long long id = 0; id < N && !any; ++id) any = (flags[size_t(id)] & cell_flag) != 0;
+  std::vector<long long> c0, c1, src, dst;
+  if (any && box_cells(L, box0, c0) && box_cells(L, box1, c1)) {
+    if (c0.size() != c1.size())
+      return report_error(FLB_ERR_INVALID, "flb_periodic_create: the boxes hold different cell counts");
+    const long long ds = (long long)L.dir_stride;
+    for (int k : comm_pop_dirs(dir0))
+      for (size_t p = 0; p < c0.size(); ++p) {
+        src.push_back(k * ds + c1[p]);
+        dst.push_back(k * ds + c0[p]);
+      }
+    for (int k : comm_pop_dirs(dir1))
+      for (size_t p = 0; p < c0.size(); ++p) {
+        src.push_back(k * ds + c0[p]);
+        dst.push_back(k * ds + c1[p]);
+      }
+  } else {
+    c0.clear();
+  }
+  flb_periodic* per = new (std::nothrow) flb_periodic();
+  if (!per) return report_error(FLB_ERR_OOM, "flb_periodic_create: host allocation");
+  per->layout = L;
+  per->npairs = (long long)c0.size();
+  per->ncopies = (long long)src.size();
+  if (per->ncopies > 0) {
+    cudaError_t e = cudaMalloc((void**)&per->d_src, src.size() * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&per->d_dst, dst.size() * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&per->d_stage, src.size() * size_t(L.elem_bytes));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(per->d_src, src.data(), src.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(per->d_dst, dst.data(), dst.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      flb_periodic_destroy(per);
+      char m[160];
+      std::snprintf(m, sizeof m, "flb_periodic_create: %s", cudaGetErrorString(e));
+      return report_error(FLB_ERR_OOM, m);
+    }
+  }
+  *out = per;
+  return FLB_OK;
+}
+
+int flb_periodic_count(const flb_periodic* per, long long* pairs, long long* copies) {
+  if (!per) return report_error(FLB_ERR_INVALID, "flb_periodic_count: null handle");
+  if (pairs) *pairs = per->npairs;
+  if (copies) *copies = per->ncopies;
+  return FLB_OK;
+}
+
+int flb_periodic_apply(flb_periodic* per, flb_lattice* lat, void* stream) {
+  if (!per || !lat) return report_error(FLB_ERR_INVALID, "flb_periodic_apply: null argument");
+  if (per->ncopies == 0) return FLB_OK;
+  flb_layout L{};
+  int rc = flb_get_layout(lat, &L);
+  if (rc) return rc;
+  if (L.nx != per->layout.nx || L.ny != per->layout.ny || L.nz != per->layout.nz ||
+      L.pitch_x != per->layout.pitch_x || L.elem_bytes != per->layout.elem_bytes ||
+      L.dir_stride != per->layout.dir_stride)
+    return report_error(FLB_ERR_INVALID, "flb_periodic_apply: lattice differs from the one at creation");
+  void* pops = nullptr;
+  if ((rc = flb_device_pointers(lat, &pops, nullptr, nullptr, nullptr))) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (L.elem_bytes == 2) return periodic_launch<unsigned short>(per, pops, st);
+  if (L.elem_bytes == 8) return periodic_launch<unsigned long long>(per, pops, st);
+  return periodic_launch<unsigned>(per, pops, st);
+}
+
+int flb_periodic_destroy(flb_periodic* per) {
+  if (!per) return FLB_OK;
+  if (per->d_src) cudaFree(per->d_src);
+  if (per->d_dst) cudaFree(per->d_dst);
+  if (per->d_stage) cudaFree(per->d_stage);
+  delete per;
+  return FLB_OK;
+}
 
 int flb_bb_create(flb_lattice* lat, uint8_t cell_flag, uint8_t void_flag, int kind, double rho0,
                   flb_bb** out) {

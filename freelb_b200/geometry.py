@@ -59,6 +59,16 @@ def uneven_blocks(ni: int, edges=(32, 48, 64, 96), seed: int = 0):
     return blocks
 
 
+def x_blocks(ni: int, cuts):
+    """Blocks tiling an ni^3 interior split along x only at the given cuts (full
+    y and z), in x order, in the form uneven_blocks returns."""
+    n = ni + 2
+    edges = [0] + list(cuts) + [ni]
+    return [{"x0": a, "y0": 0, "z0": 0, "ex": b - a, "ey": ni, "ez": ni,
+             "nx": b - a + 2, "ny": n, "nz": n, "ox": a, "oy": 0, "oz": 0}
+            for a, b in zip(edges[:-1], edges[1:])]
+
+
 def block_tuples(blocks):
     """(nx, ny, nz, ox, oy, oz) per block, the form the C ABI takes."""
     return [(b["nx"], b["ny"], b["nz"], b["ox"], b["oy"], b["oz"]) for b in blocks]

@@ -193,7 +193,7 @@ def ref_binary(dtype=np.float32):
 
 def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float32,
                   blockfile=None, threads=None, outdir=None, alpha=None, fields=None,
-                  poststream=None, comm=None):
+                  poststream=None, comm=None, periodic=False):
     """Run the reference's own CPU path; returns (dict of arrays, mlups)."""
     exe = ref_binary(dtype)
     if exe is None:
@@ -217,6 +217,8 @@ def run_reference(model, ni, tau, ulid, steps, warmup=0, cs=0.1, dtype=np.float3
         env["FLB_POSTSTREAM_BB"] = str(int(poststream))
     if comm is not None:  # "full" / "all": NormalFullCommunicate / NormalAllCommunicate
         env["FLB_COMM"] = comm
+    if periodic:  # FixedPeriodicBoundaryManager on the x = 0 / x = Ni-1 wall columns
+        env["FLB_PERIODIC"] = "1"
     args = [exe, model, str(ni), repr(float(tau)), repr(float(ulid)), str(steps), str(warmup),
             outdir, repr(float(cs))]
     if blockfile:
@@ -411,6 +413,58 @@ def poststream_bb(lat, cell_flag, void_flag, kind="normal"):
             bracket = (1.0 + sq * 0.5 * 9.0) - np.float64(norm2(uw) * T(0.5) * T(3))
             val = (np.float64(T(2) * rho * w) * bracket - np.float64(prev)).astype(lat.dtype)
         R[j, xs] = val
+
+
+def comm_pop_dirs(direction):
+    """getCommPopDir (src/parallel/communicator.h:74-150): the directions that
+    enter a cell across the faces named by the NbrDirection bits (XN=1, XP=2,
+    YN=4, YP=8, ZN=16, ZP=32), sorted."""
+    out = []
+    for i in range(19):
+        c = C[i]
+        sel = ((direction & 1 and c[0] > 0) or (direction & 2 and not direction & 1 and c[0] < 0)
+               or (direction & 4 and c[1] > 0) or (direction & 8 and not direction & 4 and c[1] < 0)
+               or (direction & 16 and c[2] > 0)
+               or (direction & 32 and not direction & 16 and c[2] < 0))
+        if sel:
+            out.append(i)
+    return out
+
+
+def box_cells(nx, ny, nz, box):
+    """Stored cells of an inclusive box (x0, x1, y0, y1, z0, z1), clamped to the
+    mesh, in z, y, x order (BasicBlock::getCellIdx, basic_geometry.hh:593-619)."""
+    x0, x1, y0, y1, z0, z1 = box
+    x0, y0, z0 = max(x0, 0), max(y0, 0), max(z0, 0)
+    x1, y1, z1 = min(x1, nx - 1), min(y1, ny - 1), min(z1, nz - 1)
+    z, y, x = np.meshgrid(np.arange(z0, z1 + 1), np.arange(y0, y1 + 1), np.arange(x0, x1 + 1),
+                          indexing="ij")
+    return (x + nx * (y + ny * z)).reshape(-1)
+
+
+def periodic_copy(lat, box0, dir0, box1, dir1):
+    """FixedPeriodicBoundaryManager::Apply (src/boundary/periodic_boundary.h:
+    302-321) on a restated single-block lattice, as the two-way exchange the
+    reference performs between boxes in different blocks: box0 cell[k] =
+    box1 cell[k] for k in getCommPopDir(dir0) and box1 cell[k] = box0 cell[k]
+    for k in getCommPopDir(dir1), on the post-collision populations.  The
+    restated step fuses collide and stream, so the copy is applied to the
+    post-stream state: a pre-stream P_k(x) sits at R_k((x + Delta_k) mod N)
+    (CyclicArray::rotate, field.h:676-697).  Sources are read before any write."""
+    nx, ny, nz, N = lat.nx, lat.ny, lat.nz, lat.N
+    R = lat.pops.reshape(19, N)
+    c0 = box_cells(nx, ny, nz, box0)
+    c1 = box_cells(nx, ny, nz, box1)
+    assert c0.size == c1.size
+    moves = []
+    for k in comm_pop_dirs(dir0):
+        d = int(C[k][0]) + nx * (int(C[k][1]) + ny * int(C[k][2]))
+        moves.append((k, (c0 + d) % N, R[k, (c1 + d) % N].copy()))
+    for k in comm_pop_dirs(dir1):
+        d = int(C[k][0]) + nx * (int(C[k][1]) + ny * int(C[k][2]))
+        moves.append((k, (c1 + d) % N, R[k, (c0 + d) % N].copy()))
+    for k, dst, val in moves:
+        R[k, dst] = val
 
 
 # ---------------------------------------------------------------------------

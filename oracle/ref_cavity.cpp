@@ -35,6 +35,15 @@
 //             the lid (8) with bounceback::movingwall and the walls (4) with
 //             bounceback::normal (k=1), anti_simple (2), anti_O1 (3),
 //             anti_O2 (4) or anti_pressure (5) (bounce_back_boundary.h:167-256).
+//   FLB_PERIODIC=1 (environment): the wall cells of the x = 0 and x = Ni-1
+//             interior columns (y, z inside [1, Nj-1] x [1, Nk-1]) take flag 16,
+//             which no task matches (no collision), and a
+//             FixedPeriodicBoundaryManager (boundary/periodic_boundary.h:136-321)
+//             on those two boxes, Setup(left, XN, right, XP), runs Apply()
+//             between ApplyCellDynamics and Stream as in
+//             examples/couette2d/couette2d.cpp:171-214.  Use a block file whose
+//             first block holds the x = 0 column and a later block the
+//             x = Ni-1 column (the manager's cross-block pairing).
 //   blockfile optional BlockReader file (io/block_reader.h) for a multi-block run;
 //             NormalCommunicate() (FLB_COMM=full / all: NormalFullCommunicate /
 //             NormalAllCommunicate) follows Stream() as in
@@ -73,6 +82,7 @@ constexpr std::uint8_t VoidFlag = std::uint8_t(1);
 constexpr std::uint8_t AABBFlag = std::uint8_t(2);
 constexpr std::uint8_t BouncebackFlag = std::uint8_t(4);
 constexpr std::uint8_t BBMovingWallFlag = std::uint8_t(8);
+constexpr std::uint8_t PeriodicFlag = std::uint8_t(16);
 
 // Per-cell Brinkman porosity for the single-block run (FLB_ALPHA_FILE).
 static std::vector<T> g_alpha;
@@ -138,6 +148,19 @@ struct Runner {
     FlagFM.forEach(toplid, [&](FLAG& field, std::size_t id) {
       if (util::isFlag(field.get(id), BouncebackFlag)) field.SetField(id, BBMovingWallFlag);
     });
+    const char* pe = std::getenv("FLB_PERIODIC");
+    const bool periodic = pe && std::atoi(pe) == 1;
+    const T nx = cavity.getMax()[0], ny = cavity.getMax()[1], nz = cavity.getMax()[2];
+    const AABB<T, 3> left(Vector<T, 3>(T(0), T(1), T(1)), Vector<T, 3>(T(1), ny - 1, nz - 1));
+    const AABB<T, 3> right(Vector<T, 3>(nx - 1, T(1), T(1)), Vector<T, 3>(nx, ny - 1, nz - 1));
+    if (periodic) {
+      FlagFM.forEach(left, [&](FLAG& field, std::size_t id) {
+        if (util::isFlag(field.get(id), BouncebackFlag)) field.SetField(id, PeriodicFlag);
+      });
+      FlagFM.forEach(right, [&](FLAG& field, std::size_t id) {
+        if (util::isFlag(field.get(id), BouncebackFlag)) field.SetField(id, PeriodicFlag);
+      });
+    }
 
     BlockLatticeManager<T, LatSet, FIELDS> NSLattice(Geo, InitValues, BaseConv);
     Vector<T, 3> U_Wall{p.ulid, T{}, T{}};
@@ -188,6 +211,9 @@ struct Runner {
       "NS_ABB4", NSLattice, FlagFM, BouncebackFlag, VoidFlag);
     BBLikeFixedBlockBdManager<bounceback::movingwall<CELL>, LM, FM> NS_BBMW(
       "NS_BBMW", NSLattice, FlagFM, BBMovingWallFlag, VoidFlag);
+    FixedPeriodicBoundaryManager<LM, FM> NS_Peri("NS_Peri", NSLattice, FlagFM, PeriodicFlag,
+                                                 VoidFlag);
+    if (periodic) NS_Peri.Setup(left, NbrDirection::XN, right, NbrDirection::XP);
     // FLB_COMM=full / all: NormalFullCommunicate / NormalAllCommunicate
     const char* cm = std::getenv("FLB_COMM");
     const int comm = cm ? (std::string(cm) == "full" ? 1 : (std::string(cm) == "all" ? 2 : 0)) : 0;
@@ -210,6 +236,7 @@ struct Runner {
         NS_BBMW.Apply();
       } else {
         NSLattice.template ApplyCellDynamics<NSTask>(FlagFM);
+        if (periodic) NS_Peri.Apply();
         NSLattice.Stream();
       }
       if (multi) {

@@ -1,6 +1,7 @@
 """Generate the golden fixtures in tests/golden/ by running the reference itself.
 
     make -C oracle && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --periodic   (the periodic-manager fixtures only)
 
 Each fixture is the output of the reference FreeLB CPU path (the harness
 oracle/ref_cavity.cpp compiled from the reference's own headers into
@@ -62,6 +63,26 @@ def multiblock(name, ni, edges, seed, steps, dtype):
     print(name, "written,", len(blocks), "blocks")
 
 
+def periodic(name, ni, cuts, steps, dtype):
+    """Reference run with FixedPeriodicBoundaryManager on the x = 0 / x = ni-1
+    wall columns (ref_cavity FLB_PERIODIC=1) over x-split blocks."""
+    import tempfile
+    from freelb_b200 import geometry as G
+    blocks = G.x_blocks(ni, cuts)  # the manager pairs a box in an earlier block with a later one
+    with tempfile.TemporaryDirectory() as d:
+        bf = os.path.join(d, "blocks.txt")
+        G.write_block_file(bf, blocks)
+        r = O.run_reference("bgk", ni, 0.6, 0.1, steps, 0, dtype=dtype, blockfile=bf,
+                            threads=4, periodic=True)
+    out = {"params": np.array([ni, 0.6, 0.1, steps], dtype=np.float64),
+           "cuts": np.array(cuts), "nblocks": np.array(len(blocks))}
+    for k in range(len(blocks)):
+        for f in ("flags", "pops"):
+            out[f"{f}_b{k}"] = r[f"{f}_b{k}"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "written,", len(blocks), "blocks")
+
+
 def c1():
     ni, steps = 100, 1000
     r = O.run_reference("bgk", ni, 0.53, 0.1, steps, 0, dtype=np.float32)
@@ -79,6 +100,10 @@ def c1():
 
 
 if __name__ == "__main__":
+    if "--periodic" in sys.argv:
+        periodic("periodic_bgk_f64_n12_s30", 12, (5,), 30, np.float64)
+        periodic("periodic_bgk_f32_n12_s30", 12, (5,), 30, np.float32)
+        sys.exit(0)
     for case in SMALL:
         small(*case)
     multiblock("blocks_bgk_f64_n12_s30", 12, (4, 8), 3, 30, np.float64)

@@ -106,3 +106,24 @@ def test_host_example_halfway_bounce_back_managers(gpu_ok):
     rrho, ru = ref.rhou_fields()
     assert rel_maxnorm(data[:N], rrho) < 1e-5
     assert rel_maxnorm(data[N:], ru) < 1e-5
+
+
+@pytest.mark.gpu
+def test_host_periodic_manager_matches_reference(gpu_ok):
+    """FixedPeriodicBoundaryManager through the host classes (AABB boxes,
+    Setup(left, XN, right, XP), Apply() between ApplyCellDynamics and Stream)
+    against the reference's own periodic run (tests/golden/periodic_*)."""
+    from freelb_b200 import build as B
+    from conftest import golden
+    from test_periodic import fluid_compare
+    B.build_examples()
+    exe = os.path.join(ROOT, "freelb_b200", "cpp", "_build", "periodic3d_b200")
+    g = golden("periodic_bgk_f32_n12_s30")
+    ni, tau, ulid, steps = (float(v) for v in g["params"])
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "out.bin")
+        r = subprocess.run([exe, str(int(ni)), str(tau), str(ulid), str(int(steps)), out],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        pops = np.fromfile(out, dtype=np.float64).astype(np.float32)
+    assert fluid_compare(g, pops, int(ni), np.float32) < 1e-5
