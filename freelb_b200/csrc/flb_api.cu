@@ -100,6 +100,8 @@ struct flb_lattice {
   StepParams sp{};
   // multi-block launch data
   BlockEntry* d_blocks = nullptr;
+  int* d_tile_block = nullptr;  // block of every tile (tile kernel)
+  long long tile_block_cap = 0;
   long long ntiles = 0;
   int table_tile_y = 0;
   int table_vec = 0;
@@ -294,6 +296,20 @@ int upload_block_table(flb_lattice* h) {
   if (!h->d_blocks) FLB_CUDA(cudaMalloc((void**)&h->d_blocks, t.size() * sizeof(BlockEntry)));
   FLB_CUDA(cudaMemcpy(h->d_blocks, t.data(), t.size() * sizeof(BlockEntry),
                       cudaMemcpyHostToDevice));
+  // tile -> block, so that a CTA finds its block with one load
+  std::vector<int> tb(static_cast<size_t>(start));
+  for (size_t b = 0; b < t.size(); ++b) {
+    const long long end = b + 1 < t.size() ? t[b + 1].tile_start : start;
+    for (long long k = t[b].tile_start; k < end; ++k) tb[size_t(k)] = int(b);
+  }
+  if (start > h->tile_block_cap) {
+    if (h->d_tile_block) cudaFree(h->d_tile_block);
+    h->d_tile_block = nullptr;
+    h->tile_block_cap = 0;
+    FLB_CUDA(cudaMalloc((void**)&h->d_tile_block, size_t(start) * sizeof(int)));
+    h->tile_block_cap = start;
+  }
+  FLB_CUDA(cudaMemcpy(h->d_tile_block, tb.data(), tb.size() * sizeof(int), cudaMemcpyHostToDevice));
   h->ntiles = start;
   h->table_tile_y = h->tile_y;
   h->table_vec = vec_width(h);
@@ -501,7 +517,7 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));
     k_pull_blocks<S, R, MODEL, V><<<unsigned(g), dim3(32 * h->tile_y), 0, st>>>(
-        h->sp, h->d_blocks, int(h->blocks.size()), h->ntiles);
+        h->sp, h->d_blocks, h->d_tile_block, h->ntiles);
   }
 }
 
@@ -878,7 +894,7 @@ int flb_destroy(flb_lattice* h) {
   if (h->alpha) cudaFree(h->alpha);
   for (void* p : {h->pops[0], h->pops[1], (void*)h->flags, h->rho, h->vel, (void*)h->acc,
                   h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo,
-                  (void*)h->d_lut})
+                  (void*)h->d_lut, (void*)h->d_tile_block})
     if (p) cudaFree(p);
   delete h;
   return FLB_OK;
@@ -937,7 +953,7 @@ int flb_memory_bytes(const flb_lattice* h, size_t* bytes) {
   const size_t ds = size_t(h->dstride);
   *bytes = 2 * size_t(Q) * ds * h->elem_bytes + ds + 4 * ds * h->real_bytes + 64 +
            h->stage_bytes + (h->uprev ? 3 * ds * sizeof(double) : 0) +
-           h->blocks.size() * sizeof(BlockEntry) +
+           h->blocks.size() * sizeof(BlockEntry) + size_t(h->tile_block_cap) * sizeof(int) +
            size_t(h->nhalo) * (h->halo32 ? sizeof(uint2) : sizeof(HaloCopy));
   return FLB_OK;
 }

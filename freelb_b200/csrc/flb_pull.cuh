@@ -775,20 +775,14 @@ __global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas) k_pull
 }
 
 // Many blocks: tiles of blockDim.x consecutive chunks, numbered block by block
-// (tile_start = first tile of the block); CTAs walk the tiles with a grid stride
-// (persistent) or take one tile each.
+// (tile_start = first tile of the block, tile_block = block of every tile);
+// CTAs walk the tiles with a grid stride (persistent) or take one tile each.
 template <typename S, typename R, int MODEL, int V>
 __global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas)
-    k_pull_blocks(const StepParams p, const BlockEntry* __restrict__ blocks, int nblocks,
-                  long long ntiles) {
+    k_pull_blocks(const StepParams p, const BlockEntry* __restrict__ blocks,
+                  const int* __restrict__ tile_block, long long ntiles) {
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    int lo = 0, hi = nblocks - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (blocks[mid].tile_start <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    const BlockEntry& b = blocks[lo];
+    const BlockEntry& b = blocks[__ldg(tile_block + t)];
     const long long q = (t - b.tile_start) * blockDim.x + threadIdx.x;
     int x0, y, z;
     if (chunk_coords<V>(b.g, q, x0, y, z))
