@@ -413,6 +413,17 @@ struct Cell {
   using FloatType = T;
   using LatticeSet = LatSet;
 };
+// The reference's device field packs and cells (benchmarks/cavity3d_cu/
+// cavity3d.cu:158-162): on this path every lattice field already lives on the
+// device, so the device pack is the field pack and the device cell the cell tag.
+template <typename FIELDS>
+struct ExtractCudevFieldPack {
+  using cudev_pack = FIELDS;
+};
+namespace cudev {
+template <typename T, typename LatSet, typename FIELDS>
+using Cell = ::Cell<T, LatSet, FIELDS>;
+}  // namespace cudev
 
 // BlockFieldManager<FLAG, T, 3> (src/data_struct/field_struct.h:39-335)
 template <typename FieldType, typename T, unsigned int Dim>
@@ -646,10 +657,18 @@ class BlockLatticeManager {
     } else if constexpr (std::is_same<F, RHO<T>>::value) {
       pull_fields();
       return rho_;
+    } else if constexpr (std::is_same<F, POP<T, 19>>::value) {
+      return pops_;
     } else {
       static_assert(sizeof(F) == 0, "field not mirrored on the host");
     }
   }
+  // getField<POP<T, 19>>(): the populations live only on the device (created
+  // at their equilibrium by the constructor), so copyToDevice() has nothing to
+  // send; read them through flb_download_pops(handle(), ...).
+  struct DevicePopulations {
+    void copyToDevice() {}
+  };
 
   // ApplyCellDynamics<TaskSelector>(FlagFM) (block_lattice.hh:766-778)
   template <typename Selector, typename FlagManager>
@@ -768,6 +787,7 @@ class BlockLatticeManager {
   bool fields_stale_ = false;
   bool tolerance_on_ = false;
   std::vector<flb_periodic*> periodic_;
+  DevicePopulations pops_;
 };
 
 // ---------------------------------------------------------------------------

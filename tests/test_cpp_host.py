@@ -10,8 +10,13 @@ import pytest
 from conftest import ROOT, rel_maxnorm
 
 REF_BENCH = "/root/reference/benchmarks/cavity3d/cavity3d.cpp"
+REF_BENCH_CU = "/root/reference/benchmarks/cavity3d_cu/cavity3d.cu"
 INC = os.path.join(ROOT, "freelb_b200", "cpp")
 LIBDIR = os.path.join(ROOT, "freelb_b200")
+# the reference's own benchmark programs built against the host classes (here,
+# where their sources are); the GPU tests run whichever of them exist
+REF_PROGRAMS = {"cpu": os.path.join(INC, "_build", "ref_cavity3d"),
+                "cu": os.path.join(INC, "_build", "ref_cavity3d_cu")}
 
 
 def _gxx(args):
@@ -26,11 +31,75 @@ def _gxx(args):
 def test_reference_benchmark_compiles_unchanged_against_host_classes():
     """benchmarks/cavity3d/cavity3d.cpp, untouched, with only the include path
     changed, compiles and links against libflb_b200.so."""
+    exe = REF_PROGRAMS["cpu"]
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    r = _gxx(["-I" + INC, REF_BENCH, "-L" + LIBDIR, "-lflb_b200", "-Wl,-rpath,$ORIGIN/../..",
+              "-o", exe])
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert os.path.exists(exe)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_BENCH_CU), reason="reference sources not present")
+def test_reference_cuda_benchmark_compiles_unchanged_against_host_classes():
+    """benchmarks/cavity3d_cu/cavity3d.cu (CuDevApplyCellDynamics / CuDevStream,
+    cudev::Cell, copyToDevice), untouched, compiles with nvcc and links against
+    libflb_b200.so with only the include path changed."""
+    exe = REF_PROGRAMS["cu"]
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    r = subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I" + INC, REF_BENCH_CU, "-L" + LIBDIR, "-lflb_b200",
+                        "-Xlinker", "-rpath,$ORIGIN/../..", "-o", exe],
+                       capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert os.path.exists(exe)
+
+
+CAVITY_INI = """[parallel]
+thread_num = 1
+block_num = 1
+[Mesh]
+Ni = 24
+Nj = 24
+Nk = 24
+Cell_Len = 1
+[Physical_Property]
+rho_ref = 1
+Kine_Visc = 0.01
+[Init_Conditions]
+U_Ini0 = 0
+U_Ini1 = 0
+U_Ini2 = 0
+U_Max = 0.1
+[Boundary_Conditions]
+Velo_Wall0 = 0.1
+Velo_Wall1 = 0
+Velo_Wall2 = 0
+[LB]
+RT = 0.53
+[Simulation_Settings]
+TotalStep = 30
+OutputStep = 10
+[tolerance]
+tol = 1e-9
+"""
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["cpu", "cu"])
+def test_reference_benchmark_programs_run_on_gpu(gpu_ok, kind):
+    """The reference's cavity3d benchmark programs (CPU and CUDA versions), built
+    unchanged against the host classes, run their main loop on the GPU."""
+    exe = REF_PROGRAMS[kind]
+    if not os.path.exists(exe):
+        pytest.skip("reference benchmark programs not built (no reference sources at build)")
     with tempfile.TemporaryDirectory() as d:
-        exe = os.path.join(d, "cavity3d")
-        r = _gxx(["-I" + INC, REF_BENCH, "-L" + LIBDIR, "-lflb_b200", "-o", exe])
-        assert r.returncode == 0, r.stderr[-3000:]
-        assert os.path.exists(exe)
+        open(os.path.join(d, "cavity3d.ini"), "w").write(CAVITY_INI)
+        r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "MLUPs" in r.stdout
 
 
 def test_host_example_compiles():
