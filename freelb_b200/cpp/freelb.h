@@ -53,6 +53,14 @@
 #include <omp.h>
 #endif
 
+// The reference's build-time float type (src/head.h:43-48: -DFLOAT_TYPE=...,
+// double by default).
+#ifdef FLOAT_TYPE
+using FLOAT = FLOAT_TYPE;
+#else
+using FLOAT = double;
+#endif
+
 // ---------------------------------------------------------------------------
 // errors
 namespace flbcpp {
@@ -216,6 +224,11 @@ inline MpiManagerStub& mpi() {
 }
 #ifndef MPI_DEBUG_WAIT
 #define MPI_DEBUG_WAIT
+#endif
+// the rank guards of src/parallel/mpi_manager.h:80-81 without MPI_ENABLED
+#ifndef MPI_RANK
+#define MPI_RANK(x)
+#define IF_MPI_RANK(x)
 #endif
 
 // ---------------------------------------------------------------------------

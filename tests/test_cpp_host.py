@@ -11,12 +11,14 @@ from conftest import ROOT, rel_maxnorm
 
 REF_BENCH = "/root/reference/benchmarks/cavity3d/cavity3d.cpp"
 REF_BENCH_CU = "/root/reference/benchmarks/cavity3d_cu/cavity3d.cu"
+REF_EXAMPLE = "/root/reference/examples/cavity3d/cavity3d.cpp"
 INC = os.path.join(ROOT, "freelb_b200", "cpp")
 LIBDIR = os.path.join(ROOT, "freelb_b200")
 # the reference's own benchmark programs built against the host classes (here,
 # where their sources are); the GPU tests run whichever of them exist
 REF_PROGRAMS = {"cpu": os.path.join(INC, "_build", "ref_cavity3d"),
-                "cu": os.path.join(INC, "_build", "ref_cavity3d_cu")}
+                "cu": os.path.join(INC, "_build", "ref_cavity3d_cu"),
+                "example": os.path.join(INC, "_build", "ref_example_cavity3d")}
 
 
 def _gxx(args):
@@ -57,6 +59,18 @@ def test_reference_cuda_benchmark_compiles_unchanged_against_host_classes():
     assert os.path.exists(exe)
 
 
+@pytest.mark.skipif(not os.path.exists(REF_EXAMPLE), reason="reference sources not present")
+def test_reference_cavity3d_example_compiles_unchanged_against_host_classes():
+    """examples/cavity3d/cavity3d.cpp (post-stream bounce-back managers, vtmo
+    writers, getToleranceU, NormalCommunicate, the MPI rank guards), untouched,
+    compiles and links against the host classes."""
+    exe = REF_PROGRAMS["example"]
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    r = _gxx(["-I" + INC, REF_EXAMPLE, "-L" + LIBDIR, "-lflb_b200", "-Wl,-rpath,$ORIGIN/../..",
+              "-o", exe])
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
 CAVITY_INI = """[parallel]
 thread_num = 1
 block_num = 1
@@ -65,6 +79,7 @@ Ni = 24
 Nj = 24
 Nk = 24
 Cell_Len = 1
+BlockCellLen = 8
 [Physical_Property]
 rho_ref = 1
 Kine_Visc = 0.01
@@ -88,10 +103,11 @@ tol = 1e-9
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["cpu", "cu"])
+@pytest.mark.parametrize("kind", ["cpu", "cu", "example"])
 def test_reference_benchmark_programs_run_on_gpu(gpu_ok, kind):
-    """The reference's cavity3d benchmark programs (CPU and CUDA versions), built
-    unchanged against the host classes, run their main loop on the GPU."""
+    """The reference's cavity3d programs (the CPU and CUDA benchmarks and the
+    cavity3d example), built unchanged against the host classes, run their main
+    loop on the GPU."""
     exe = REF_PROGRAMS[kind]
     if not os.path.exists(exe):
         pytest.skip("reference benchmark programs not built (no reference sources at build)")
