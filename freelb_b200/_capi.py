@@ -113,6 +113,16 @@ SIGNATURES = {
     "flb_periodic_apply": [_P, _P, _P],
     "flb_periodic_destroy": [_P],
     "flb_set_halo_mode": [_P, _I],
+    "flb_exchange_plan": [_I, ctypes.POINTER(BlockDesc), ctypes.POINTER(_I), _I, _I, _I,
+                          ctypes.POINTER(_I), ctypes.POINTER(_I),
+                          ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+    "flb_exchange_create": [_P, _I, ctypes.POINTER(BlockDesc), ctypes.POINTER(_I), _I,
+                            ctypes.POINTER(_P)],
+    "flb_exchange_peers": [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
+    "flb_exchange_pack": [_P, _P, _I, _P, _P],
+    "flb_exchange_unpack": [_P, _P, _I, _P, _P],
+    "flb_exchange_destroy": [_P],
     "flb_vtk_field_base64": [_P, _I, _I, _I, _I, _I, ctypes.c_double, ctypes.c_double,
                              ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), _P],
 }

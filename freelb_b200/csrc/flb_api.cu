@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 #include <type_traits>
@@ -926,6 +927,268 @@ int flb_set_tasks(flb_lattice* h, int ntasks, const uint8_t* keys, const uint8_t
 int flb_block_count(const flb_lattice* h, int* n) {
   if (!h || !n) return fail(FLB_ERR_INVALID, "null argument");
   *n = int(h->blocks.size());
+  return FLB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Exchange between ranks: the global halo records whose two blocks have
+// different owners.
+
+namespace {
+
+struct ExchPeer {
+  int rank = -1;
+  std::vector<long long> send, recv;  // element offsets (direction included)
+  long long* d_send = nullptr;
+  long long* d_recv = nullptr;
+};
+
+// Enumerate the global records in canonical order (block k, overlap cell
+// z-y-x, direction) and hand every cross-rank one to `fn(k, lx, ly, lz, o, i)`
+// (destination block k, local cell of k; source block o owning that cell).
+template <typename F>
+int for_each_cross_record(int nglobal, const flb_block_desc* blocks, const int* owner_rank,
+                          int halo_mode, F&& fn) {
+  int gx = 0, gy = 0, gz = 0;
+  for (int k = 0; k < nglobal; ++k) {
+    const flb_block_desc& b = blocks[k];
+    if (b.ox < 0 || b.oy < 0 || b.oz < 0 || b.nx < 3 || b.ny < 3 || b.nz < 3)
+      return fail(FLB_ERR_INVALID, "global block %d: bad extent or origin", k);
+    gx = std::max(gx, b.ox + b.nx);
+    gy = std::max(gy, b.oy + b.ny);
+    gz = std::max(gz, b.oz + b.nz);
+  }
+  const long long gn = (long long)gx * gy * gz;
+  if (gn > (1LL << 33)) return fail(FLB_ERR_INVALID, "global block extent too large");
+  std::vector<int> owner(size_t(gn), -1);
+  for (int k = 0; k < nglobal; ++k) {
+    const flb_block_desc& b = blocks[k];
+    for (int z = b.oz + 1; z < b.oz + b.nz - 1; ++z)
+      for (int y = b.oy + 1; y < b.oy + b.ny - 1; ++y)
+        for (int x = b.ox + 1; x < b.ox + b.nx - 1; ++x) {
+          int& o = owner[size_t((long long)(z * (long long)gy + y) * gx + x)];
+          if (o >= 0) return fail(FLB_ERR_INVALID, "blocks %d and %d overlap in their interiors", o, k);
+          o = k;
+        }
+  }
+  const bool full = halo_mode == FLB_HALO_FULL;
+  for (int k = 0; k < nglobal; ++k) {
+    const flb_block_desc& b = blocks[k];
+    for (int lz = 0; lz < b.nz; ++lz)
+      for (int ly = 0; ly < b.ny; ++ly)
+        for (int lx = 0; lx < b.nx; ++lx) {
+          if (lx > 0 && ly > 0 && lz > 0 && lx < b.nx - 1 && ly < b.ny - 1 && lz < b.nz - 1)
+            continue;
+          const int o = owner[size_t((long long)((b.oz + lz) * (long long)gy + (b.oy + ly)) * gx +
+                                     (b.ox + lx))];
+          if (o < 0 || owner_rank[o] == owner_rank[k]) continue;
+          const int l[3] = {lx, ly, lz};
+          const int m[3] = {b.nx, b.ny, b.nz};
+          for (int i = full ? 0 : 1; i < Q; ++i) {
+            const int c[3] = {cx(i), cy(i), cz(i)};
+            bool cross = false;
+            for (int a = 0; a < 3; ++a)
+              if ((l[a] == 0 && c[a] > 0) || (l[a] == m[a] - 1 && c[a] < 0)) cross = true;
+            if (!cross && !full) continue;
+            fn(k, lx, ly, lz, o, i);
+          }
+        }
+  }
+  return FLB_OK;
+}
+
+template <typename E>
+__global__ void k_exch_gather(const long long* __restrict__ idx, long long n, const E* pops,
+                              E* buf) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x)
+    buf[r] = pops[idx[r]];
+}
+template <typename E>
+__global__ void k_exch_scatter(const long long* __restrict__ idx, long long n, const E* buf,
+                               E* pops) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x)
+    pops[idx[r]] = buf[r];
+}
+
+}  // namespace
+
+struct flb_exchange {
+  int my_rank = 0;
+  int elem_bytes = 4;
+  long long dstride = 0;
+  std::vector<ExchPeer> peers;  // sorted by rank
+};
+
+namespace {
+ExchPeer* find_peer(flb_exchange* ex, int rank) {
+  for (ExchPeer& p : ex->peers)
+    if (p.rank == rank) return &p;
+  return nullptr;
+}
+template <typename E>
+void exch_launch(const long long* idx, long long n, const void* src, void* dst, bool gather,
+                 cudaStream_t st) {
+  const unsigned grid = unsigned(std::min<long long>(n / 256 + 1, 4096));
+  if (gather)
+    k_exch_gather<E><<<grid, 256, 0, st>>>(idx, n, static_cast<const E*>(src),
+                                           static_cast<E*>(dst));
+  else
+    k_exch_scatter<E><<<grid, 256, 0, st>>>(idx, n, static_cast<const E*>(src),
+                                            static_cast<E*>(dst));
+}
+int exch_move(flb_exchange* ex, flb_lattice* h, int peer, void* buf, bool pack, void* stream) {
+  if (!ex || !h || !buf) return fail(FLB_ERR_INVALID, "null argument");
+  if (h->dstride != ex->dstride || h->elem_bytes != ex->elem_bytes)
+    return fail(FLB_ERR_INVALID, "lattice differs from the one the exchange was built for");
+  ExchPeer* p = find_peer(ex, peer);
+  if (!p) return fail(FLB_ERR_INVALID, "rank %d is not a peer of rank %d", peer, ex->my_rank);
+  const long long n = pack ? (long long)p->send.size() : (long long)p->recv.size();
+  if (n == 0) return FLB_OK;
+  const long long* idx = pack ? p->d_send : p->d_recv;
+  cudaStream_t st = as_stream(stream);
+  void* pops = h->pops[h->cur];
+  const void* src = pack ? pops : buf;
+  void* dst = pack ? buf : pops;
+  if (ex->elem_bytes == 2) exch_launch<unsigned short>(idx, n, src, dst, pack, st);
+  else if (ex->elem_bytes == 8) exch_launch<unsigned long long>(idx, n, src, dst, pack, st);
+  else exch_launch<unsigned>(idx, n, src, dst, pack, st);
+  FLB_CUDA(cudaGetLastError());
+  return FLB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int flb_exchange_plan(int nglobal, const flb_block_desc* blocks, const int* owner_rank,
+                      int my_rank, int halo_mode, int max_peers, int* npeers, int* peer_ranks,
+                      long long* send_counts, long long* recv_counts) {
+  if (nglobal < 1 || !blocks || !owner_rank || !npeers)
+    return fail(FLB_ERR_INVALID, "flb_exchange_plan: bad arguments");
+  std::map<int, std::pair<long long, long long>> cnt;  // peer -> (send, recv)
+  FLB_TRY(for_each_cross_record(nglobal, blocks, owner_rank, halo_mode,
+                                [&](int k, int, int, int, int o, int) {
+                                  if (owner_rank[k] == my_rank) ++cnt[owner_rank[o]].second;
+                                  if (owner_rank[o] == my_rank) ++cnt[owner_rank[k]].first;
+                                }));
+  *npeers = int(cnt.size());
+  if (int(cnt.size()) > max_peers)
+    return fail(FLB_ERR_INVALID, "flb_exchange_plan: %d peers > max_peers %d", int(cnt.size()),
+                max_peers);
+  int j = 0;
+  for (const auto& kv : cnt) {
+    if (peer_ranks) peer_ranks[j] = kv.first;
+    if (send_counts) send_counts[j] = kv.second.first;
+    if (recv_counts) recv_counts[j] = kv.second.second;
+    ++j;
+  }
+  return FLB_OK;
+}
+
+int flb_exchange_create(flb_lattice* h, int nglobal, const flb_block_desc* blocks,
+                        const int* owner_rank, int my_rank, flb_exchange** out) {
+  if (!h || !out || nglobal < 1 || !blocks || !owner_rank)
+    return fail(FLB_ERR_INVALID, "flb_exchange_create: bad arguments");
+  *out = nullptr;
+  // the handle's blocks must be the ones my_rank owns, in global order
+  std::vector<int> local(size_t(nglobal), -1);
+  int nl = 0;
+  for (int k = 0; k < nglobal; ++k) {
+    if (owner_rank[k] != my_rank) continue;
+    if (nl >= int(h->blocks.size()))
+      return fail(FLB_ERR_INVALID, "rank %d owns more blocks than the handle holds", my_rank);
+    const HostBlock& hb = h->blocks[size_t(nl)];
+    const flb_block_desc& b = blocks[k];
+    if (hb.L.nx != b.nx || hb.L.ny != b.ny || hb.L.nz != b.nz || hb.ox != b.ox ||
+        hb.oy != b.oy || hb.oz != b.oz)
+      return fail(FLB_ERR_INVALID, "handle block %d differs from global block %d", nl, k);
+    local[size_t(k)] = nl++;
+  }
+  if (nl != int(h->blocks.size()))
+    return fail(FLB_ERR_INVALID, "the handle holds %d blocks, rank %d owns %d",
+                int(h->blocks.size()), my_rank, nl);
+  std::map<int, ExchPeer> peers;
+  FLB_TRY(for_each_cross_record(
+      nglobal, blocks, owner_rank, h->halo_mode, [&](int k, int lx, int ly, int lz, int o, int i) {
+        if (owner_rank[k] == my_rank) {  // receive into block k's overlap slot
+          ExchPeer& p = peers[owner_rank[o]];
+          const Geom g = geom_of(h->blocks[size_t(local[size_t(k)])]);
+          p.recv.push_back(i * h->dstride + host_wrap_src(g, lx, ly, lz, i));
+        }
+        if (owner_rank[o] == my_rank) {  // send from block o's interior slot
+          ExchPeer& p = peers[owner_rank[k]];
+          const HostBlock& hb = h->blocks[size_t(local[size_t(o)])];
+          const flb_block_desc& bk = blocks[k];
+          p.send.push_back(i * h->dstride + host_wrap_src(geom_of(hb), bk.ox + lx - hb.ox,
+                                                          bk.oy + ly - hb.oy,
+                                                          bk.oz + lz - hb.oz, i));
+        }
+      }));
+  flb_exchange* ex = new (std::nothrow) flb_exchange();
+  if (!ex) return fail(FLB_ERR_OOM, "flb_exchange_create: host allocation");
+  ex->my_rank = my_rank;
+  ex->elem_bytes = h->elem_bytes;
+  ex->dstride = h->dstride;
+  for (auto& kv : peers) {
+    kv.second.rank = kv.first;
+    ex->peers.push_back(std::move(kv.second));
+  }
+  for (ExchPeer& p : ex->peers) {
+    cudaError_t e = cudaSuccess;
+    if (!p.send.empty()) {
+      e = cudaMalloc((void**)&p.d_send, p.send.size() * sizeof(long long));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(p.d_send, p.send.data(), p.send.size() * sizeof(long long),
+                       cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess && !p.recv.empty()) {
+      e = cudaMalloc((void**)&p.d_recv, p.recv.size() * sizeof(long long));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(p.d_recv, p.recv.data(), p.recv.size() * sizeof(long long),
+                       cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+      flb_exchange_destroy(ex);
+      return fail(FLB_ERR_OOM, "flb_exchange_create: %s", cudaGetErrorString(e));
+    }
+  }
+  *out = ex;
+  return FLB_OK;
+}
+
+int flb_exchange_peers(const flb_exchange* ex, int max_peers, int* npeers, int* peer_ranks,
+                       long long* send_counts, long long* recv_counts) {
+  if (!ex || !npeers) return fail(FLB_ERR_INVALID, "null argument");
+  *npeers = int(ex->peers.size());
+  if (*npeers > max_peers)
+    return fail(FLB_ERR_INVALID, "%d peers > max_peers %d", *npeers, max_peers);
+  for (size_t j = 0; j < ex->peers.size(); ++j) {
+    if (peer_ranks) peer_ranks[j] = ex->peers[j].rank;
+    if (send_counts) send_counts[j] = (long long)ex->peers[j].send.size();
+    if (recv_counts) recv_counts[j] = (long long)ex->peers[j].recv.size();
+  }
+  return FLB_OK;
+}
+
+int flb_exchange_pack(flb_exchange* ex, flb_lattice* h, int peer, void* buf, void* stream) {
+  return exch_move(ex, h, peer, buf, true, stream);
+}
+
+int flb_exchange_unpack(flb_exchange* ex, flb_lattice* h, int peer, const void* buf,
+                        void* stream) {
+  return exch_move(ex, h, peer, const_cast<void*>(buf), false, stream);
+}
+
+int flb_exchange_destroy(flb_exchange* ex) {
+  if (!ex) return FLB_OK;
+  for (ExchPeer& p : ex->peers) {
+    if (p.d_send) cudaFree(p.d_send);
+    if (p.d_recv) cudaFree(p.d_recv);
+  }
+  delete ex;
   return FLB_OK;
 }
 

@@ -153,6 +153,37 @@ FLB_API int flb_halo_count(const flb_lattice* lat, long long* nrecords);
 #define FLB_HALO_FULL 1
 FLB_API int flb_set_halo_mode(flb_lattice* lat, int mode);
 
+/* Blocks on several GPUs (one process per GPU).  The domain is a global list
+ * of blocks, each owned by a rank; a rank's handle is an FLB_BLOCKS_HALO handle
+ * holding the blocks it owns, in global order.  The handle's own halo copies
+ * between its local blocks after each step; the records whose source block
+ * lives on another rank (the same NormalCommunicate / NormalFullCommunicate
+ * copies, block_lattice.hh:1419-1503) become per-peer exchanges: after
+ * flb_step, flb_exchange_pack gathers the populations a peer needs into a
+ * device buffer, the caller moves the buffers (NCCL send / recv), and
+ * flb_exchange_unpack scatters a peer's buffer into the overlap slots, before
+ * the next flb_step.  Every rank enumerates the global records in the same
+ * order (block, overlap cell z-y-x, direction), so a sender's buffer matches
+ * its receiver's slots element for element.  Buffers hold storage elements
+ * (2 / 4 / 8 bytes for FP16S / FP32 / FP64).
+ *
+ * flb_exchange_plan is host-only (no device or handle): the peers of my_rank
+ * and the element counts it sends to and receives from each, sorted by peer
+ * rank; max_peers bounds the output arrays. */
+typedef struct flb_exchange flb_exchange;
+FLB_API int flb_exchange_plan(int nglobal, const flb_block_desc* blocks, const int* owner_rank,
+                              int my_rank, int halo_mode, int max_peers, int* npeers,
+                              int* peer_ranks, long long* send_counts, long long* recv_counts);
+FLB_API int flb_exchange_create(flb_lattice* lat, int nglobal, const flb_block_desc* blocks,
+                                const int* owner_rank, int my_rank, flb_exchange** out);
+FLB_API int flb_exchange_peers(const flb_exchange* ex, int max_peers, int* npeers,
+                               int* peer_ranks, long long* send_counts, long long* recv_counts);
+FLB_API int flb_exchange_pack(flb_exchange* ex, flb_lattice* lat, int peer_rank, void* device_buf,
+                              void* stream);
+FLB_API int flb_exchange_unpack(flb_exchange* ex, flb_lattice* lat, int peer_rank,
+                                const void* device_buf, void* stream);
+FLB_API int flb_exchange_destroy(flb_exchange* ex);
+
 /* Rebind the per-flag task list and the bulk model (the NSTask type of
  * ApplyCellDynamics<NSTask>, src/utils/tmp.h:283-309): tasks are tried in order,
  * a cell takes the op of the first task whose key shares a bit with its flag. */
