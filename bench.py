@@ -535,12 +535,26 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="headline and e2e only (no variants / accuracy / blocks / ensemble / "
                          "adjoint blocks)")
+    ap.add_argument("--only", default=None, choices=["blocks", "ensemble"],
+                    help="run one secondary workload alone and print its JSON (profiling): "
+                         "the 48 uneven blocks of the 256^3 cavity or the 128-cavity ensemble")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.only:
+        import torch
+        import freelb_b200 as F
+        torch.cuda.set_device(local_rank)
+        stream = torch.cuda.current_stream()
+        if args.only == "blocks":
+            out = {"blocks_256": blocks_block(F, torch, stream, 256, args.steps)}
+        else:
+            out = {"ensemble_128": ensemble_block(F, torch, stream, args.steps)}
+        print(json.dumps(out), flush=True)
         return
     run_ours(args, rank, world, local_rank)
 
