@@ -1019,6 +1019,7 @@ __global__ void k_exch_scatter(const long long* __restrict__ idx, long long n, c
 struct flb_exchange {
   int my_rank = 0;
   int elem_bytes = 4;
+  int halo_mode = FLB_HALO_NORMAL;  // the handle's mode the plan was built for
   long long dstride = 0;
   std::vector<ExchPeer> peers;  // sorted by rank
 };
@@ -1044,6 +1045,8 @@ int exch_move(flb_exchange* ex, flb_lattice* h, int peer, void* buf, bool pack, 
   if (!ex || !h || !buf) return fail(FLB_ERR_INVALID, "null argument");
   if (h->dstride != ex->dstride || h->elem_bytes != ex->elem_bytes)
     return fail(FLB_ERR_INVALID, "lattice differs from the one the exchange was built for");
+  if (h->halo_mode != ex->halo_mode)
+    return fail(FLB_ERR_STATE, "halo mode changed after flb_exchange_create: rebuild the exchange");
   ExchPeer* p = find_peer(ex, peer);
   if (!p) return fail(FLB_ERR_INVALID, "rank %d is not a peer of rank %d", peer, ex->my_rank);
   const long long n = pack ? (long long)p->send.size() : (long long)p->recv.size();
@@ -1131,6 +1134,7 @@ int flb_exchange_create(flb_lattice* h, int nglobal, const flb_block_desc* block
   if (!ex) return fail(FLB_ERR_OOM, "flb_exchange_create: host allocation");
   ex->my_rank = my_rank;
   ex->elem_bytes = h->elem_bytes;
+  ex->halo_mode = h->halo_mode;
   ex->dstride = h->dstride;
   for (auto& kv : peers) {
     kv.second.rank = kv.first;

@@ -167,6 +167,9 @@ FLB_API int flb_set_halo_mode(flb_lattice* lat, int mode);
  * its receiver's slots element for element.  Buffers hold storage elements
  * (2 / 4 / 8 bytes for FP16S / FP32 / FP64).
  *
+ * The plan follows the handle's halo mode at creation (flb_set_halo_mode
+ * first); pack / unpack refuse a handle whose mode changed since.
+ *
  * flb_exchange_plan is host-only (no device or handle): the peers of my_rank
  * and the element counts it sends to and receives from each, sorted by peer
  * rank; max_peers bounds the output arrays. */
