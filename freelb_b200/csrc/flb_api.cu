@@ -611,14 +611,13 @@ int pops_transfer(flb_lattice* h, const HostBlock& B, void* host, bool upload, c
   const LayoutParams& L = B.L;
   const size_t hb = sizeof(H);
   const size_t N = size_t(L.nx) * L.ny * L.nz;
-  FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
+  FLB_TRY(ensure_stage(h, N * sizeof(H)));
   S* pops = static_cast<S*>(h->pops[h->cur]);
   const Geom g = geom_of(B);
   for (int i = 0; i < Q; ++i) {
     char* hp = static_cast<char*>(host) + i * N * hb;
     if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(h->stage, L.pitch * hb, hp, L.nx * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
+      FLB_CUDA(cudaMemcpyAsync(h->stage, hp, N * hb, cudaMemcpyHostToDevice, st));
       k_unstream_in<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
           L, g, static_cast<const H*>(h->stage), pops + i * h->dstride, i, h->sp.shift[i],
           h->sp.scale);
@@ -626,8 +625,7 @@ int pops_transfer(flb_lattice* h, const HostBlock& B, void* host, bool upload, c
       k_stream_out<S, R, H><<<grid_1d(B.padded()), 256, 0, st>>>(
           L, g, static_cast<H*>(h->stage), pops + i * h->dstride, i, h->sp.shift[i],
           h->sp.inv_scale);
-      FLB_CUDA(cudaMemcpy2DAsync(hp, L.nx * hb, h->stage, L.pitch * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+      FLB_CUDA(cudaMemcpyAsync(hp, h->stage, N * hb, cudaMemcpyDeviceToHost, st));
     }
     FLB_CUDA(cudaGetLastError());
   }
@@ -659,34 +657,26 @@ int field_transfer(flb_lattice* h, const HostBlock& B, int field, void* host, bo
   R* vel = static_cast<R*>(h->vel) + B.base;
   if (field == FLB_FIELD_ALPHA && !h->alpha)
     return fail(FLB_ERR_STATE, "no ALPHA field: the lattice model is not BRINKMAN");
+  // host order staged contiguously: one bus copy per transfer, padding on the device
+  const size_t N = size_t(L.nx) * L.ny * L.nz;
+  const int grid = grid_1d((long long)N);
   if (field == FLB_FIELD_RHO || field == FLB_FIELD_ALPHA) {
-    const bool direct = std::is_same<R, H>::value;
-    if (!direct) FLB_TRY(ensure_stage(h, size_t(B.padded()) * sizeof(H)));
-    void* dev = direct ? static_cast<void*>(rho) : h->stage;
+    FLB_TRY(ensure_stage(h, N * hb));
     if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(dev, L.pitch * hb, host, L.nx * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      if (!direct)
-        k_convert<H, R><<<grid_1d(B.padded()), 256, 0, st>>>(
-            B.padded(), static_cast<const H*>(h->stage), rho);
+      FLB_CUDA(cudaMemcpyAsync(h->stage, host, N * hb, cudaMemcpyHostToDevice, st));
+      k_pad<H, R><<<grid, 256, 0, st>>>(L, static_cast<const H*>(h->stage), rho);
     } else {
-      if (!direct)
-        k_convert<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(B.padded(), rho,
-                                                             static_cast<H*>(h->stage));
-      FLB_CUDA(cudaMemcpy2DAsync(host, L.nx * hb, dev, L.pitch * hb, L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+      k_unpad<R, H><<<grid, 256, 0, st>>>(L, rho, static_cast<H*>(h->stage));
+      FLB_CUDA(cudaMemcpyAsync(host, h->stage, N * hb, cudaMemcpyDeviceToHost, st));
     }
   } else if (field == FLB_FIELD_VELOCITY) {
-    FLB_TRY(ensure_stage(h, 3 * size_t(B.padded()) * sizeof(H)));
+    FLB_TRY(ensure_stage(h, 3 * N * hb));
     if (upload) {
-      FLB_CUDA(cudaMemcpy2DAsync(h->stage, 3 * L.pitch * hb, host, 3 * L.nx * hb, 3 * L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-      k_vel_in<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(L, static_cast<const H*>(h->stage),
-                                                          vel);
+      FLB_CUDA(cudaMemcpyAsync(h->stage, host, 3 * N * hb, cudaMemcpyHostToDevice, st));
+      k_vel_in<R, H><<<grid, 256, 0, st>>>(L, static_cast<const H*>(h->stage), vel);
     } else {
-      k_vel_out<R, H><<<grid_1d(B.padded()), 256, 0, st>>>(L, static_cast<H*>(h->stage), vel);
-      FLB_CUDA(cudaMemcpy2DAsync(host, 3 * L.nx * hb, h->stage, 3 * L.pitch * hb, 3 * L.nx * hb,
-                                 size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+      k_vel_out<R, H><<<grid, 256, 0, st>>>(L, static_cast<H*>(h->stage), vel);
+      FLB_CUDA(cudaMemcpyAsync(host, h->stage, 3 * N * hb, cudaMemcpyDeviceToHost, st));
     }
   } else {
     return fail(FLB_ERR_INVALID, "unknown field %d", field);
@@ -718,12 +708,17 @@ int flags_any(flb_lattice* h, int b, uint8_t* host, bool upload, void* stream) {
   const HostBlock& B = h->blocks[b];
   const LayoutParams& L = B.L;
   cudaStream_t st = as_stream(stream);
-  if (upload)
-    FLB_CUDA(cudaMemcpy2DAsync(h->flags + B.base, L.pitch, host, L.nx, L.nx,
-                               size_t(L.ny) * L.nz, cudaMemcpyHostToDevice, st));
-  else
-    FLB_CUDA(cudaMemcpy2DAsync(host, L.nx, h->flags + B.base, L.pitch, L.nx,
-                               size_t(L.ny) * L.nz, cudaMemcpyDeviceToHost, st));
+  const size_t N = size_t(L.nx) * L.ny * L.nz;
+  FLB_TRY(ensure_stage(h, N));
+  uint8_t* stage = static_cast<uint8_t*>(h->stage);
+  if (upload) {
+    FLB_CUDA(cudaMemcpyAsync(stage, host, N, cudaMemcpyHostToDevice, st));
+    k_pad<uint8_t, uint8_t><<<grid_1d((long long)N), 256, 0, st>>>(L, stage, h->flags + B.base);
+  } else {
+    k_unpad<uint8_t, uint8_t><<<grid_1d((long long)N), 256, 0, st>>>(L, h->flags + B.base, stage);
+    FLB_CUDA(cudaMemcpyAsync(host, stage, N, cudaMemcpyDeviceToHost, st));
+  }
+  FLB_CUDA(cudaGetLastError());
   FLB_CUDA(cudaStreamSynchronize(st));
   return FLB_OK;
 }

@@ -163,28 +163,48 @@ __global__ void k_convert(long long n, const A* in, B* out) {
     out[c] = B(in[c]);
 }
 
-// AoS velocity staging (3*pitch per row) <-> SoA planes
-template <typename R, typename H>
-__global__ void k_vel_in(LayoutParams L, const H* stage, R* vel) {
-  const long long total = L.plane * L.nz;
+// Host order (x fastest, nx values per row, contiguous) <-> the padded rows of
+// a block, with the element conversion A -> B: transfers stage the host
+// array contiguously on the device so that each crosses the bus as one copy.
+template <typename A, typename B>
+__global__ void k_pad(LayoutParams L, const A* in, B* out) {
+  const long long total = (long long)L.nx * L.ny * L.nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
        c += (long long)gridDim.x * blockDim.x) {
-    const long long row = c / L.pitch, x = c - row * L.pitch;
-    const long long s = row * 3 * L.pitch + 3 * x;
+    const long long r = c / L.nx, x = c - r * L.nx;
+    out[r * L.pitch + x] = B(in[c]);
+  }
+}
+template <typename A, typename B>
+__global__ void k_unpad(LayoutParams L, const A* in, B* out) {
+  const long long total = (long long)L.nx * L.ny * L.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    const long long r = c / L.nx, x = c - r * L.nx;
+    out[c] = B(in[r * L.pitch + x]);
+  }
+}
+
+// AoS velocity staging (host order, 3 values per cell) <-> SoA planes
+template <typename R, typename H>
+__global__ void k_vel_in(LayoutParams L, const H* stage, R* vel) {
+  const long long total = (long long)L.nx * L.ny * L.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
+       c += (long long)gridDim.x * blockDim.x) {
+    const long long r = c / L.nx, p = r * L.pitch + (c - r * L.nx);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) vel[c + d * L.dstride] = R(stage[s + d]);
+    for (int d = 0; d < 3; ++d) vel[p + d * L.dstride] = R(stage[3 * c + d]);
   }
 }
 
 template <typename R, typename H>
 __global__ void k_vel_out(LayoutParams L, H* stage, const R* vel) {
-  const long long total = L.plane * L.nz;
+  const long long total = (long long)L.nx * L.ny * L.nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
        c += (long long)gridDim.x * blockDim.x) {
-    const long long row = c / L.pitch, x = c - row * L.pitch;
-    const long long s = row * 3 * L.pitch + 3 * x;
+    const long long r = c / L.nx, p = r * L.pitch + (c - r * L.nx);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) stage[s + d] = H(vel[c + d * L.dstride]);
+    for (int d = 0; d < 3; ++d) stage[3 * c + d] = H(vel[p + d * L.dstride]);
   }
 }
 

@@ -793,7 +793,7 @@ __global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas)
 // ---------------------------------------------------------------------------
 // Transfers and helpers in R = stream(P) space.
 
-// population array i: R (staging, host dtype, padded layout) -> P slots
+// population array i: R (staging, host dtype, host order) -> P slots
 template <typename S, typename R, typename H>
 __global__ void k_unstream_in(LayoutParams L, Geom g, const H* stage, S* pops_i, int i,
                               float shift, float scale) {
@@ -802,7 +802,8 @@ __global__ void k_unstream_in(LayoutParams L, Geom g, const H* stage, S* pops_i,
        c += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
-    Storage<S, R>::store(pops_i + wrap_src(g, x, y, z, i), R(stage[c]), shift, scale);
+    Storage<S, R>::store(pops_i + wrap_src(g, x, y, z, i),
+                         R(stage[((long long)z * L.ny + y) * L.nx + x]), shift, scale);
   }
 }
 
@@ -814,7 +815,8 @@ __global__ void k_stream_out(LayoutParams L, Geom g, H* stage, const S* pops_i, 
        c += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
-    stage[c] = H(Storage<S, R>::load(pops_i + wrap_src(g, x, y, z, i), shift, inv_scale));
+    stage[((long long)z * L.ny + y) * L.nx + x] =
+        H(Storage<S, R>::load(pops_i + wrap_src(g, x, y, z, i), shift, inv_scale));
   }
 }
 
