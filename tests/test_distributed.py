@@ -163,3 +163,16 @@ def test_emulated_ranks_full_halo_equal_multiblock(gpu_ok):
         a = rl.lat.download_pops(block=kl).reshape(19, -1)
         w = whole.lat.download_pops(block=k).reshape(19, -1)
         assert np.array_equal(a[:, fb != 1], w[:, fb != 1]), k
+
+
+@pytest.mark.gpu
+def test_exchange_rejects_a_handle_that_does_not_match(gpu_ok):
+    blocks = D.slabs(12, 2)
+    with pytest.raises(F.FlbError):  # rank 1's handle built from rank 0's block
+        wrong = [b if k == 0 else blocks[0] for k, b in enumerate(blocks)]
+        rl = D.RankLattice(wrong, [0, 1], 1, 0.6)
+    rl = D.RankLattice(blocks, [0, 1], 0, 0.6)
+    rl.lat.set_halo_mode("full")  # the plan was built for the normal halo
+    with pytest.raises(F.FlbError):
+        rl.pack()
+    rl.close()

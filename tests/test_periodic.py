@@ -135,3 +135,13 @@ def test_device_periodic_rules(gpu_ok):
     # a box outside the interior: empty
     out = F.PeriodicBoundaryManager(lat, (0, 0, 0, 0, 0, 0), "XN", b1, "XP", 16)
     assert out.counts() == (0, 0)
+
+
+@pytest.mark.gpu
+def test_periodic_rejects_multiblock_handles(gpu_ok):
+    from freelb_b200 import geometry as G
+    blocks = x_blocks(8, (4,))
+    lat = F.Lattice.blocks(G.block_tuples(blocks), 0.6, mode="halo")
+    b0, b1 = boxes(8)
+    with pytest.raises(F.FlbError):
+        F.PeriodicBoundaryManager(lat, b0, "XN", b1, "XP", 16)
