@@ -271,13 +271,7 @@ int upload_op_lut(flb_lattice* h) {
 // boundaries (nx rounded up to 16); narrow blocks, where that padding would
 // idle a large share of the lanes, round up to 4 only (the vector loads need
 // 16-byte alignment at most).
-int row_pitch(int nx) {
-#ifdef FLB_PITCH_ALWAYS_16
-  return (nx + 15) / 16 * 16;
-#else
-  return nx >= 240 ? (nx + 15) / 16 * 16 : (nx + 3) / 4 * 4;
-#endif
-}
+int row_pitch(int nx) { return nx >= 240 ? (nx + 15) / 16 * 16 : (nx + 3) / 4 * 4; }
 
 // Block table for the tile kernel (rebuilt when tile_y changes).
 int upload_block_table(flb_lattice* h) {
