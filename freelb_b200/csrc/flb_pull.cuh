@@ -937,13 +937,32 @@ __global__ void k_halo_pull(const HaloCopy* __restrict__ recs, long long n, S* p
 
 // The same copies as (source, destination) element indices into the whole
 // population buffer, 8 bytes per record instead of 24, when 19 x dstride <
-// 2^32; records sorted by destination.
+// 2^32; records sorted by destination.  A thread takes HALO_BATCH records a
+// grid stride apart and issues all their record loads, then all their
+// gathers, then all their stores: the x-face gathers each miss to DRAM, and
+// one outstanding gather per thread leaves the memory system idle.  Sources
+// are interior cells and destinations overlap cells, so no record reads what
+// another writes and the order inside a thread does not matter.
+constexpr int HALO_BATCH = 4;
+
 template <typename S>
 __global__ void k_halo_pull32(const uint2* __restrict__ recs, long long n, S* pops) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
-       r += (long long)gridDim.x * blockDim.x) {
-    const uint2 h = __ldg(recs + r);
-    pops[h.y] = pops[h.x];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; r0 < n;
+       r0 += stride * HALO_BATCH) {
+    uint2 h[HALO_BATCH];
+    S v[HALO_BATCH];
+#pragma unroll
+    for (int k = 0; k < HALO_BATCH; ++k) {
+      const long long r = r0 + k * stride;
+      h[k] = r < n ? __ldg(recs + r) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < HALO_BATCH; ++k)
+      if (r0 + k * stride < n) v[k] = pops[h[k].x];
+#pragma unroll
+    for (int k = 0; k < HALO_BATCH; ++k)
+      if (r0 + k * stride < n) pops[h[k].y] = v[k];
   }
 }
 
