@@ -1,10 +1,12 @@
 // flb_kernels.cuh -- fused stream-and-collide and helper kernels (sm_100a).
 //
 // HBM layout of one block lattice (all arrays padded the same way):
-//   cell (x,y,z) -> x + y*pitch + z*plane, pitch = nx rounded up to 32
-//   elements (rows start on 128-byte boundaries for FP32), plane = pitch*ny;
+//   cell (x,y,z) -> base + x + y*pitch + z*plane, pitch = nx rounded up to 16
+//   elements for nx >= 240 (rows start on 64-byte boundaries for FP32) and to
+//   4 below (row_pitch in flb_api.cu), plane = pitch*ny; each block starts at
+//   `base`, the sum of the blocks before it rounded up to 64 elements each;
 //   population i lives at pops + i*dstride + cell (structure of arrays), with
-//   dstride = plane*nz rounded up to 64 elements.
+//   dstride = the whole padded lattice.
 // The reference keeps the same SoA split (GenericFieldBase, field.h:1419-1575)
 // on an unpadded mesh; padding is invisible at the C ABI, which converts to
 // and from the reference's linear order on upload/download.
