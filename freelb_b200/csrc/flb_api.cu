@@ -154,6 +154,14 @@ int grid_1d(long long n) {
   return int(b < 1 ? 1 : b);
 }
 
+// k_halo_pull32: enough 256-thread CTAs for one batch of HALO_BATCH records
+// per thread, so that no thread starts a second, mostly idle, round.
+int halo32_grid(long long n) {
+  const long long per_cta = 256LL * HALO_BATCH;
+  const long long b = (n + per_cta - 1) / per_cta;
+  return int(std::min(std::max(b, 1LL), 1LL << 20));
+}
+
 int validate_common(const flb_lattice_desc* d) {
   if (!d) return fail(FLB_ERR_INVALID, "null descriptor");
   if (d->storage < 0 || d->storage > 2) return fail(FLB_ERR_INVALID, "bad storage %d", d->storage);
@@ -528,7 +536,7 @@ void launch_one_step(flb_lattice* h, cudaStream_t st) {
   }
   if (h->nhalo > 0) {
     if (h->halo32)
-      k_halo_pull32<S><<<grid_1d(h->nhalo), 256, 0, st>>>(
+      k_halo_pull32<S><<<halo32_grid(h->nhalo), 256, 0, st>>>(
           reinterpret_cast<const uint2*>(h->d_halo), h->nhalo, static_cast<S*>(h->sp.dst));
     else
       k_halo_pull<S><<<grid_1d(h->nhalo), 256, 0, st>>>(h->d_halo, h->nhalo,
