@@ -489,6 +489,19 @@ StepParams half_step_params(const flb_lattice* h) {
   return p;
 }
 
+// Direction bases of the multi-block FP16S tile kernel: src + i * dstride and
+// dst + i * dstride (blocks differ in their row steps, which the kernel adds).
+StepParams block_half_params(const flb_lattice* h) {
+  StepParams p = h->sp;
+  const __half* src = static_cast<const __half*>(p.src);
+  __half* dst = static_cast<__half*>(p.dst);
+  for (int i = 0; i < Q; ++i) {
+    p.src_dir[i] = src + i * p.dstride;
+    p.dst_dir[i] = dst + i * p.dstride;
+  }
+  return p;
+}
+
 template <typename S, typename R, int MODEL, int V>
 void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
   if constexpr (std::is_same<S, __half>::value && V == PIPE_V && MODEL != MODEL_BRINKMAN) {
@@ -519,6 +532,13 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
   } else {
     long long g = h->ctas_per_sm > 0 ? (long long)h->ctas_per_sm * h->sm_count : h->ntiles;
     g = std::max(1LL, std::min(g, h->ntiles));
+    if constexpr (std::is_same<S, __half>::value && V >= 2) {
+      if ((long long)Q * h->dstride < (1LL << 32)) {
+        k_pull_blocks_half32<MODEL, V><<<unsigned(g), dim3(32 * h->tile_y), 0, st>>>(
+            block_half_params(h), h->d_blocks, h->d_tile_block, h->ntiles);
+        return;
+      }
+    }
     k_pull_blocks<S, R, MODEL, V><<<unsigned(g), dim3(32 * h->tile_y), 0, st>>>(
         h->sp, h->d_blocks, h->d_tile_block, h->ntiles);
   }

@@ -694,6 +694,75 @@ __device__ __forceinline__ void pull_chunk_half32(const StepParams& p, const Geo
 }
 
 // One chunk: the thread owns cells x0 .. x0+V-1 of row (y, z), x0 < nx.
+// Multi-block FP16S chunk with 32-bit element offsets (19 x dstride < 2^32).
+// Blocks differ in pitch and plane, so the direction bases carry no row
+// offset here: p.src_dir[i] = src + i * dstride, p.dst_dir[i] = dst + i *
+// dstride, and the source of direction i is its base plus the chunk's cell
+// index moved by -c_y pitch - c_z plane.  On interior rows every such index
+// lies inside the block, so the unsigned offsets never wrap.  The loads, the
+// splices and the collision are those of gather_words / collide_store_half,
+// so the result is the same bit for bit; only the addressing differs (no
+// 64-bit row pointers live across the gather).
+template <int V>
+__device__ __forceinline__ void gather_words_blk(const StepParams& p, const Geom& g, int x0,
+                                                 unsigned cell,
+                                                 typename HWord<V>::type (&h)[Q]) {
+  using W = typename HWord<V>::type;
+  const unsigned pitch = unsigned(g.pitch), plane = unsigned(g.plane);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const unsigned sc = cell - unsigned(cy(i)) * pitch - unsigned(cz(i)) * plane;
+    const __half* own = static_cast<const __half*>(p.src_dir[i]) + sc;
+    const W v = hload<V>(own);
+    if (cx(i) == 0) {
+      h[i] = v;
+    } else if (cx(i) > 0) {
+      h[i] = hsplice_prev(hload<V>(x0 >= V ? own - V : own), v);
+    } else {
+      h[i] = hsplice_next(v, hload<V>(x0 + V < g.nx ? own + V : own));
+    }
+  }
+  if (x0 == 0) {  // x = nx-1 of the row before the source row
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+      if (cx(i) > 0) {
+        const unsigned e = cell - unsigned(cy(i)) * pitch - unsigned(cz(i)) * plane - pitch +
+                           unsigned(g.nx - 1);
+        hset(h[i], 0, hscalar(static_cast<const __half*>(p.src_dir[i]) + e));
+      }
+  }
+  const int klast = g.nx - 1 - x0;
+  if (klast >= 0 && klast < V) {  // x = 0 of the row after the source row
+#pragma unroll
+    for (int i = 1; i < Q; ++i)
+      if (cx(i) < 0) {
+        const unsigned e = cell - unsigned(cy(i)) * pitch - unsigned(cz(i)) * plane + pitch -
+                           unsigned(x0);
+        const unsigned w = hscalar(static_cast<const __half*>(p.src_dir[i]) + e);
+#pragma unroll
+        for (int k = 0; k < V; ++k)
+          if (k == klast) hset(h[i], k, w);
+      }
+  }
+}
+
+template <int MODEL, int V>
+__device__ __forceinline__ void pull_chunk_half_blk32(const StepParams& p, const Geom& g,
+                                                      float omega, int x0, int y, int z) {
+  typename HWord<V>::type h[Q];
+  const unsigned cell = unsigned(g.base) + unsigned(y) * unsigned(g.pitch) +
+                        unsigned(z) * unsigned(g.plane) + unsigned(x0);
+  if (interior_row(g, y, z))
+    gather_words_blk<V>(p, g, x0, cell, h);
+  else
+    gather_words_wrap<V>(static_cast<const __half*>(p.src), p.dstride, g, x0, y, z, h);
+  uint8_t fl[V];
+  load_flags<V>(p.flags + cell, fl);
+  collide_half<MODEL, V>(p, omega, (long long)cell, fl, h);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) hstore<V>(static_cast<__half*>(p.dst_dir[i]) + cell, h[i]);
+}
+
 template <typename S, typename R, int MODEL, int V>
 __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R omega, int lane,
                                            int x0, int y, int z) {
@@ -787,6 +856,20 @@ __global__ void __launch_bounds__(256, PullBounds<S, MODEL, V>::min_ctas)
     int x0, y, z;
     if (chunk_coords<V>(b.g, q, x0, y, z))
       pull_chunk<S, R, MODEL, V>(p, b.g, R(b.omega), 0, x0, y, z);
+  }
+}
+
+// k_pull_blocks for FP16S storage with 32-bit offsets (pull_chunk_half_blk32).
+template <int MODEL, int V>
+__global__ void __launch_bounds__(256, PullBounds<__half, MODEL, V>::min_ctas)
+    k_pull_blocks_half32(const StepParams p, const BlockEntry* __restrict__ blocks,
+                         const int* __restrict__ tile_block, long long ntiles) {
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BlockEntry& b = blocks[__ldg(tile_block + t)];
+    const long long q = (t - b.tile_start) * blockDim.x + threadIdx.x;
+    int x0, y, z;
+    if (chunk_coords<V>(b.g, q, x0, y, z))
+      pull_chunk_half_blk32<MODEL, V>(p, b.g, float(b.omega), x0, y, z);
   }
 }
 

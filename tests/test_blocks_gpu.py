@@ -12,10 +12,11 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def gpu_blocks(ni, blocks, storage="fp32", tau=0.53, ulid=0.1):
+def gpu_blocks(ni, blocks, storage="fp32", tau=0.53, ulid=0.1, model="bgk"):
     n = ni + 2
     flags = F.cavity_flags(ni)
-    lat = F.Lattice.blocks(G.block_tuples(blocks), tau, mode="halo", storage=storage)
+    lat = F.Lattice.blocks(G.block_tuples(blocks), tau, mode="halo", storage=storage,
+                           model=model)
     real = lat.real
     u = np.zeros((n ** 3, 3), dtype=real)
     u[flags == 8, 0] = real(ulid)
@@ -64,6 +65,27 @@ def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas, vec):
         fb = G.slice_block(F.cavity_flags(ni), n, b).reshape(b["nz"], b["ny"], b["nx"])
         ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
         assert np.array_equal(pb[:, fb == 2], ps[:, fb == 2])
+
+
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+@pytest.mark.parametrize("tile_y,ctas,vec", [(8, 0, 4), (2, 8, 2), (4, 16, 4)])
+def test_fp16s_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, model, tile_y, ctas, vec):
+    """FP16S storage: the multi-block tile kernel (32-bit offsets) and the
+    single-block kernel give the same bits on fluid cells."""
+    ni = 40
+    blocks = G.uneven_blocks(ni, edges=(8, 12, 16), seed=7)
+    lat = gpu_blocks(ni, blocks, "fp16s", tau=0.55, model=model)
+    lat.set_launch(tile_y, ctas, vec)
+    lat.step(30)
+    one = F.cavity(ni, tau=0.55, storage="fp16s", model=model)
+    one.step(30)
+    n = ni + 2
+    P = one.download_pops().reshape(19, n, n, n)
+    for k, b in enumerate(blocks):
+        pb = lat.download_pops(block=k).reshape(19, b["nz"], b["ny"], b["nx"])
+        fb = G.slice_block(F.cavity_flags(ni), n, b).reshape(b["nz"], b["ny"], b["nx"])
+        ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
+        assert np.array_equal(pb[:, fb == 2], ps[:, fb == 2]), (model, k)
 
 
 def test_blocks_vs_oracle_multiblock_fp64(gpu_ok):
