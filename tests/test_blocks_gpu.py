@@ -190,7 +190,7 @@ def test_vector_widths_are_bitwise_equal(gpu_ok, storage, widths, ni):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5), ("fp16s", 2e-3)])
 def test_full_halo_matches_oracle(gpu_ok, storage, tol):
     """flb_set_halo_mode(FULL): all 19 populations of every overlap cell from its
     owner (NormalFullCommunicate / NormalAllCommunicate), against the oracle's
@@ -202,7 +202,7 @@ def test_full_halo_matches_oracle(gpu_ok, storage, tol):
     lat.set_halo_mode("full")
     assert lat.halo_count() > normal
     lat.step(steps)
-    dt = np.float64 if storage == "fp64" else np.float32
+    dt = np.float32 if storage == "fp32" else np.float64  # FP16S against FP64
     mb = O.MultiBlock(blocks, O.cavity_flags(ni), ni + 2, dtype=dt, full=True)
     mb.step(steps)
     pops = np.concatenate([lat.download_pops(block=k) for k in range(len(blocks))])
