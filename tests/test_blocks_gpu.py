@@ -127,6 +127,24 @@ def test_ensemble_each_cavity_matches_single(gpu_ok, graph):
         assert rel_maxnorm(lat.download_pops(block=k), ref.pops) < 1e-5, (k, n, t)
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_fp16s_ensemble_each_cavity_equals_single(gpu_ok, graph):
+    """FP16S storage: the batched cavities, each with its own tau, give the bits
+    of one FP16S handle per cavity (the 32-bit tile kernel against the
+    single-block kernel)."""
+    rng = np.random.default_rng(2)
+    sizes = [int(v) for v in rng.integers(6, 24, size=7)]
+    taus = [0.5 + 3 * 0.1 * n / float(np.exp(rng.uniform(np.log(100), np.log(3000))))
+            for n in sizes]
+    lat = ensemble(sizes, taus, storage="fp16s")
+    lat.step(25, graph=graph)
+    for k, (n, t) in enumerate(zip(sizes, taus)):
+        one = F.cavity(n, tau=t, ulid=0.1, storage="fp16s")
+        one.step(25)
+        assert np.array_equal(lat.download_pops(block=k), one.download_pops()), (k, n, t)
+        one.close()
+
+
 def test_graph_step_equals_plain_step(gpu_ok):
     a = F.cavity(30)
     b = F.cavity(30)
