@@ -15,7 +15,8 @@ import numpy as np
 from . import _capi as C
 from ._capi import FlbError  # noqa: F401
 
-STORAGES = {"fp32": C.STORAGE_FP32, "fp16s": C.STORAGE_FP16S, "fp64": C.STORAGE_FP64}
+STORAGES = {"fp32": C.STORAGE_FP32, "fp16s": C.STORAGE_FP16S, "fp64": C.STORAGE_FP64,
+            "fp32s": C.STORAGE_FP32S}
 MODELS = {"bgk": C.MODEL_BGK, "mrt": C.MODEL_MRT, "les": C.MODEL_LES,
           "brinkman": C.MODEL_BRINKMAN}
 FIELDS = {"rho": C.FIELD_RHO, "u": C.FIELD_VELOCITY, "alpha": C.FIELD_ALPHA}

@@ -15,7 +15,7 @@ FLB_OK = 0
 ERRORS = {-1: "FLB_ERR_INVALID", -2: "FLB_ERR_CUDA", -3: "FLB_ERR_OOM", -4: "FLB_ERR_TIMEOUT",
           -5: "FLB_ERR_NUMERIC", -6: "FLB_ERR_UNSUPPORTED", -7: "FLB_ERR_STATE"}
 
-STORAGE_FP32, STORAGE_FP16S, STORAGE_FP64 = 0, 1, 2
+STORAGE_FP32, STORAGE_FP16S, STORAGE_FP64, STORAGE_FP32S = 0, 1, 2, 3
 MODEL_BGK, MODEL_MRT, MODEL_LES, MODEL_BRINKMAN = 0, 1, 2, 3
 OP_NONE, OP_BULK, OP_BOUNCEBACK, OP_MOVINGWALL, OP_FIELD_BGK = 0, 1, 2, 3, 4
 DTYPE_F32, DTYPE_F64 = 0, 1

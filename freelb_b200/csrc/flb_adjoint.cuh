@@ -43,19 +43,17 @@ struct AdjParams {
 };
 
 // Transposed Jacobian of a bulk MRT cell (see above).  s: per-moment rate over
-// |M_k|^2 as the forward step uses it.
+// |M_k|^2 as the forward step uses it.  The state enters as rho, u and the
+// non-equilibrium part n = f - feq.
 template <typename R>
-__device__ __forceinline__ void mrt_vjp(const R* f, const R* mu, R* lam, R omega, const R* s,
-                                        double& gtau) {
-  R rho, ux, uy, uz, feq[Q];
-  rho_u(f, rho, ux, uy, uz);
-  feq2(feq, rho, ux, uy, uz);
+__device__ __forceinline__ void mrt_vjp(R rho, R ux, R uy, R uz, const R* n, const R* mu, R* lam,
+                                        R omega, const R* s, double& gtau) {
   R am[9], bm[9], an[9], bn[9];
 #pragma unroll
   for (int p = 0; p < 9; ++p) {
     am[p] = mu[2 * p + 1] + mu[2 * p + 2];
     bm[p] = mu[2 * p + 1] - mu[2 * p + 2];
-    const R n1 = f[2 * p + 1] - feq[2 * p + 1], n2 = f[2 * p + 2] - feq[2 * p + 2];
+    const R n1 = n[2 * p + 1], n2 = n[2 * p + 2];
     an[p] = n1 + n2;
     bn[p] = n1 - n2;
   }
@@ -64,8 +62,8 @@ __device__ __forceinline__ void mrt_vjp(const R* f, const R* mu, R* lam, R omega
 #pragma unroll
   for (int k = 0; k < Q; ++k)
     if (mrt_shear(k))
-      gt += double(mrt_moment<R>(k, mu[0], am, bm)) *
-            double(mrt_moment<R>(k, f[0] - feq[0], an, bn)) / double(mrt_norm_lit(k));
+      gt += double(mrt_moment<R>(k, mu[0], am, bm)) * double(mrt_moment<R>(k, n[0], an, bn)) /
+            double(mrt_norm_lit(k));
   gtau += double(omega) * double(omega) * gt;
   // nu = A mu, from the forward relaxation applied to zero
   R nu[Q];
@@ -114,8 +112,9 @@ __device__ __forceinline__ void mrt_vjp(const R* f, const R* mu, R* lam, R omega
   }
 }
 
-// Transposed Jacobian of one cell.  f: R_t of the cell, mu in, lam out.
-template <typename R, int MODEL>
+// Transposed Jacobian of one cell.  f: R_t of the cell as stored (DEV: the
+// FP32S deviations f - rho0 w), mu in, lam out.
+template <typename R, int MODEL, bool DEV>
 __device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f, const R* mu,
                                          R* lam, R omega, R alpha, R rho_w, double& gtau,
                                          double& gulid, double& galpha) {
@@ -145,11 +144,28 @@ __device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f
 #pragma unroll
     for (int k = 0; k < Q; ++k)
       s[k] = mrt_shear(k) ? omega * (R(1) / R(mrt_norm_lit(k))) : R(p.s_over_norm[k]);
-    mrt_vjp<R>(f, mu, lam, omega, s, gtau);
+    R rho, ux, uy, uz, n[Q];
+    if constexpr (DEV) {
+      R delta, den;
+      dev_moments(reinterpret_cast<const float(&)[Q]>(*f), p.rho0, 0.0f, delta, rho, den, ux, uy,
+                  uz);
+      dev_neq(reinterpret_cast<const float(&)[Q]>(*f), delta, rho, ux, uy, uz, n);
+    } else {
+      R feq[Q];
+      rho_u(f, rho, ux, uy, uz);
+      feq2(feq, rho, ux, uy, uz);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) n[i] = f[i] - feq[i];
+    }
+    mrt_vjp<R>(rho, ux, uy, uz, n, mu, lam, omega, s, gtau);
     return;
   }
-  R rho, den, ux, uy, uz;
-  forced_moments(f, alpha, rho, den, ux, uy, uz);
+  R rho, den, ux, uy, uz, delta = R(0);
+  if constexpr (DEV)
+    dev_moments(reinterpret_cast<const float(&)[Q]>(*f), p.rho0, alpha, delta, rho, den, ux, uy,
+                uz);
+  else
+    forced_moments(f, alpha, rho, den, ux, uy, uz);
   const R u2 = ux * ux + uy * uy + uz * uz;
   const R fo = R(1) - R(0.5) * omega;
   // The sums over i above need only the weighted moments of mu:
@@ -193,9 +209,16 @@ __device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f
   const R bx = A * M1x + B * Pux - Cc * M0 * ux;
   const R by = A * M1y + B * Puy - Cc * M0 * uy;
   const R bz = A * M1z + B * Puz - Cc * M0 * uz;
-  R sR = 0;
+  R sR = 0;  // sum mu f (DEV: sum mu d)
 #pragma unroll
   for (int i = 0; i < Q; ++i) sR += mu[i] * f[i];
+  // sum mu (feq - f); DEV, with f = d + rho0 w and sum mu rho0 w = rho0 M0:
+  // delta M0 + rho (feq_sum - M0) - sum mu d, all of deviation size
+  double s_neq;
+  if constexpr (DEV)
+    s_neq = double(delta * M0 + rho * (R(3) * M1u + R(4.5) * uPu - R(1.5) * u2 * M0)) - double(sR);
+  else
+    s_neq = double(sF) - double(sR);
   const R inv_den = R(1) / den;
   const R ub = bx * ux + by * uy + bz * uz;
   // lambda_j = (1-w) mu_j + w sum mu feq / rho + (c_j - u).b / den
@@ -210,12 +233,13 @@ __device__ __forceinline__ void cell_vjp(const StepParams& p, int op, const R* f
     if (cz(j) > 0) cb += qz; else if (cz(j) < 0) cb -= qz;
     lam[j] = c1 * mu[j] + cb;
   }
-  gtau += -double(omega) * double(omega) * (double(sF) - double(sR) - 0.5 * double(sG));
+  gtau += -double(omega) * double(omega) * (s_neq - 0.5 * double(sG));
   galpha += double(-ub * R(0.5) * inv_den) + double(fo) * double(sGa);
 }
 
-// One backward step over a single block: lam_out = J_C^T S^T lam_in.
-template <typename R, int V, int MODEL>
+// One backward step over a single block: lam_out = J_C^T S^T lam_in.  DEV: the
+// forward states are FP32S deviations (read as stored).
+template <typename R, int V, int MODEL, bool DEV>
 __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const AdjParams a) {
   const Geom g{p.nx, p.ny, p.nz, p.pitch, p.plane, 0};
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -249,7 +273,7 @@ __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const 
         const int op = select_op(p, fl[k]);
         const R al = alpha ? alpha[cell0 + k] : R(0);
         const R rw = op == OP_MBB ? rho[cell0 + k] : R(1);
-        cell_vjp<R, MODEL>(p, op, f, m, l, omega, al, rw, gtau, gulid, ga);
+        cell_vjp<R, MODEL, DEV>(p, op, f, m, l, omega, al, rw, gtau, gulid, ga);
         if (op == OP_BULK && alpha) a.galpha[cell0 + k] += ga;
       } else {
 #pragma unroll
@@ -288,10 +312,12 @@ __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const 
 // Objective J = sum_{bulk cells} |u|^2 at the current state, its seed
 // lambda_T = dJ/dR_T and the direct term dJ/dalpha = -|u|^2 / (rho + alpha/2).
 // With seed == false only J is accumulated (finite-difference evaluations).
+// CTA b writes its share of J to partials[b]; k_sum_partials adds them in a
+// fixed order, so J is the same bits on every evaluation of the same state.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const S* pops,
                                                    StepParams sp, R* lam, double* galpha,
-                                                   double* jacc, bool seed) {
+                                                   double* partials, bool seed) {
   double jsum = 0;
   const long long total = L.plane * L.nz;
   const R* alpha = static_cast<const R*>(sp.alpha);
@@ -307,10 +333,16 @@ __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const
       continue;
     }
     R f[Q];
-    gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
     const R al = alpha ? alpha[c] : R(0);
     R rho, den, ux, uy, uz;
-    forced_moments(f, al, rho, den, ux, uy, uz);
+    if constexpr (std::is_same<S, dev32>::value) {
+      R delta;
+      gather_stored<S, R>(pops, L.dstride, g, x, y, z, sp, f);
+      dev_moments(f, sp.rho0, al, delta, rho, den, ux, uy, uz);
+    } else {
+      gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
+      forced_moments(f, al, rho, den, ux, uy, uz);
+    }
     const R u2 = ux * ux + uy * uy + uz * uz;
     jsum += double(u2);
     if (seed) {
@@ -322,7 +354,14 @@ __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const
     }
   }
   jsum = warp_sum(jsum);
-  if ((threadIdx.x & 31) == 0 && jsum != 0.0) atomicAdd(jacc, jsum);
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = jsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) v += red[w];
+    partials[blockIdx.x] = v;
+  }
 }
 
 }  // namespace flb

@@ -94,6 +94,7 @@ struct flb_lattice {
   void* rho = nullptr;
   void* vel = nullptr;
   double* acc = nullptr;
+  double* red = nullptr;  // per-CTA partial sums of the FP64 reductions (RED_SLOTS x 4)
   void* stage = nullptr;
   size_t stage_bytes = 0;
   double* uprev = nullptr;
@@ -127,6 +128,11 @@ struct flb_lattice {
   double* adj_gpart = nullptr;  // per-thread-block dJ/dtau, dJ/du_lid sums
   size_t adj_gpart_n = 0;
 };
+
+// Storage kind of a handle, for the library's other translation units.
+namespace flb {
+int lattice_storage(const flb_lattice* h) { return h->desc.storage; }
+}  // namespace flb
 
 namespace {
 
@@ -164,7 +170,7 @@ int halo32_grid(long long n) {
 
 int validate_common(const flb_lattice_desc* d) {
   if (!d) return fail(FLB_ERR_INVALID, "null descriptor");
-  if (d->storage < 0 || d->storage > 2) return fail(FLB_ERR_INVALID, "bad storage %d", d->storage);
+  if (d->storage < 0 || d->storage > 3) return fail(FLB_ERR_INVALID, "bad storage %d", d->storage);
   if (d->model < 0 || d->model > 3) return fail(FLB_ERR_INVALID, "bad model %d", d->model);
   if (d->model == FLB_MODEL_BRINKMAN && d->storage == FLB_STORAGE_FP16S)
     return fail(FLB_ERR_UNSUPPORTED, "BRINKMAN model is built for FP32 and FP64 storage");
@@ -240,10 +246,12 @@ void build_params(flb_lattice* h) {
     const double w = i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
     p.shift[i] = float(d.rho0 * w);
   }
-  // 2^10: keeps deviations down to ~6e-8 out of the binary16 subnormal range
-  // while leaving headroom to |f - w| = 64.
-  p.scale = 1024.0f;
-  p.inv_scale = 1.0f / 1024.0f;
+  // FP16S: 2^10 keeps deviations down to ~6e-8 out of the binary16 subnormal
+  // range while leaving headroom to |f - w| = 64.  FP32S stores the deviations
+  // unscaled.
+  const bool fp32s = d.storage == FLB_STORAGE_FP32S;
+  p.scale = fp32s ? 1.0f : 1024.0f;
+  p.inv_scale = fp32s ? 1.0f : 1.0f / 1024.0f;
   p.rho0 = float(d.rho0);
 }
 
@@ -415,6 +423,7 @@ int with_types(flb_lattice* h, F&& f) {
   switch (h->desc.storage) {
     case FLB_STORAGE_FP32: return f((float*)nullptr, (float*)nullptr);
     case FLB_STORAGE_FP16S: return f((__half*)nullptr, (float*)nullptr);
+    case FLB_STORAGE_FP32S: return f((dev32*)nullptr, (float*)nullptr);
     default: return f((double*)nullptr, (double*)nullptr);
   }
 }
@@ -786,6 +795,7 @@ int create_common(const flb_lattice_desc* desc, std::vector<HostBlock> blocks, i
       (e = cudaMalloc(&h->vel, 3 * ds * h->real_bytes)) != cudaSuccess ||
       (e = cudaMalloc((void**)&h->acc, 64)) != cudaSuccess ||
       (e = cudaMemset(h->acc, 0, 64)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&h->red, RED_SLOTS * 4 * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc((void**)&h->d_lut, 256)) != cudaSuccess)
     return cleanup(fail(FLB_ERR_OOM, "cudaMalloc fields: %s", cudaGetErrorString(e)));
   if (desc->model == FLB_MODEL_BRINKMAN) {
@@ -911,6 +921,7 @@ int flb_destroy(flb_lattice* h) {
   flb_adjoint_release(h);
   if (h->alpha) cudaFree(h->alpha);
   for (void* p : {h->pops[0], h->pops[1], (void*)h->flags, h->rho, h->vel, (void*)h->acc,
+                  (void*)h->red,
                   h->stage, (void*)h->uprev, (void*)h->d_blocks, (void*)h->d_halo,
                   (void*)h->d_lut, (void*)h->d_tile_block})
     if (p) cudaFree(p);
@@ -1472,9 +1483,11 @@ int flb_reduce_conservation(flb_lattice* h, uint8_t key, double out[4], void* st
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
     return for_blocks(h, [&](const HostBlock& b) {
-      k_conservation_pull<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->acc,
+      const int grid = grid_1d(b.padded());
+      k_conservation_pull<S, R><<<grid, 256, 0, st>>>(
+          b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->flags, key, h->red,
           h->sp);
+      k_sum_partials<<<1, 256, 0, st>>>(h->red, grid, 4, h->acc);  // blocks in order
       return FLB_OK;
     });
   }));
@@ -1559,7 +1572,7 @@ int flb_objective_u2(flb_lattice* h, double* J, void* stream) {
   if (!h || !J) return fail(FLB_ERR_INVALID, "null argument");
   if (h->blocks.size() != 1) return fail(FLB_ERR_UNSUPPORTED, "objective on single-block handles");
   if (h->desc.storage == FLB_STORAGE_FP16S)
-    return fail(FLB_ERR_UNSUPPORTED, "objective is built for FP32 and FP64 storage");
+    return fail(FLB_ERR_UNSUPPORTED, "objective is built for FP32, FP32S and FP64 storage");
   cudaStream_t st = as_stream(stream);
   double* jacc = h->acc + 4;
   FLB_CUDA(cudaMemsetAsync(jacc, 0, sizeof(double), st));
@@ -1567,10 +1580,13 @@ int flb_objective_u2(flb_lattice* h, double* J, void* stream) {
   int rc = with_types(h, [&](auto* sp, auto* rp) {
     using S = std::remove_pointer_t<decltype(sp)>;
     using R = std::remove_pointer_t<decltype(rp)>;
-    if constexpr (!std::is_same<S, __half>::value)
-      k_objective<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+    if constexpr (!std::is_same<S, __half>::value) {
+      const int grid = grid_1d(b.padded());
+      k_objective<S, R><<<grid, 256, 0, st>>>(
           b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->sp, (R*)nullptr,
-          (double*)nullptr, jacc, false);
+          (double*)nullptr, h->red, false);
+      k_sum_partials<<<1, 256, 0, st>>>(h->red, grid, 1, jacc);
+    }
     return FLB_OK;
   });
   if (rc) return rc;
@@ -1604,7 +1620,7 @@ static int adjoint_supported(flb_lattice* h) {
   if (h->blocks.size() != 1 || h->mode >= 0)
     return fail(FLB_ERR_UNSUPPORTED, "the adjoint runs on single-block handles");
   if (h->desc.storage == FLB_STORAGE_FP16S)
-    return fail(FLB_ERR_UNSUPPORTED, "the adjoint is built for FP32 and FP64 storage");
+    return fail(FLB_ERR_UNSUPPORTED, "the adjoint is built for FP32, FP32S and FP64 storage");
   if (h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_BRINKMAN &&
       h->desc.model != FLB_MODEL_MRT)
     return fail(FLB_ERR_UNSUPPORTED, "the adjoint covers BGK, BRINKMAN and MRT bulk models");
@@ -1619,10 +1635,14 @@ int flb_adjoint_forward(flb_lattice* h, int nsteps, int every, double* J, void* 
   FLB_TRY(adjoint_supported(h));
   if (nsteps < 1 || every < 1) return fail(FLB_ERR_INVALID, "nsteps and checkpoint_every >= 1");
   cudaStream_t st = as_stream(stream);
-  flb_adjoint_release(h);
   const size_t bytes = size_t(Q) * size_t(h->dstride) * h->elem_bytes;
   const int nck = (nsteps + every - 1) / every;
-  for (int c = 0; c < nck; ++c) {
+  // a previous pair of the same shape leaves its buffers for this one (no
+  // allocation when gradients are evaluated repeatedly); any other shape
+  // starts afresh
+  if ((int)h->adj_ckpt.size() != nck || (int)h->adj_seg.size() != every - 1)
+    flb_adjoint_release(h);
+  for (int c = int(h->adj_ckpt.size()); c < nck; ++c) {
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
@@ -1661,10 +1681,11 @@ int flb_adjoint_forward(flb_lattice* h, int nsteps, int every, double* J, void* 
 
 }  // extern "C"
 
-template <typename R>
+template <typename S, typename R>
 static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau,
                               double* dJ_dulid, cudaStream_t st) {
   constexpr int V = std::is_same<R, double>::value ? 1 : 2;
+  constexpr bool DEV = std::is_same<S, dev32>::value;  // forward states are FP32S deviations
   const HostBlock& b = h->blocks[0];
   const size_t ds = size_t(h->dstride);
   const size_t qbytes = size_t(Q) * ds * h->elem_bytes;
@@ -1681,12 +1702,10 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
       return fail(FLB_ERR_OOM, "recompute slot (%zu bytes): %s", qbytes, cudaGetErrorString(e));
     h->adj_seg.push_back(p);
   }
-  double* jacc = h->acc + 4;
-  FLB_CUDA(cudaMemsetAsync(h->acc + 4, 0, sizeof(double), st));
-  // seed lambda_T = dJ/dR_T and the direct dJ/dalpha term
-  k_objective<R, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-      b.L, geom_of(b), static_cast<const R*>(h->pops[h->cur]), h->sp,
-      static_cast<R*>(h->adj_lam[0]), h->alpha ? h->adj_galpha : nullptr, jacc, true);
+  // seed lambda_T = dJ/dR_T and the direct dJ/dalpha term (the J partials are unused)
+  k_objective<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
+      b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->sp,
+      static_cast<R*>(h->adj_lam[0]), h->alpha ? h->adj_galpha : nullptr, h->red, true);
   FLB_CUDA(cudaGetLastError());
   int cur = 0;
   const long long chunks = (long long)(b.L.pitch / V) * b.L.ny * b.L.nz;
@@ -1720,9 +1739,9 @@ static int adjoint_backward_t(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau
       a.lam_out = h->adj_lam[cur ^ 1];
       a.q = q[t - t0];
       if (h->desc.model == FLB_MODEL_MRT)
-        k_adjoint_step<R, V, MODEL_MRT><<<grid, block, 0, st>>>(h->sp, a);
+        k_adjoint_step<R, V, MODEL_MRT, DEV><<<grid, block, 0, st>>>(h->sp, a);
       else
-        k_adjoint_step<R, V, MODEL_BGK><<<grid, block, 0, st>>>(h->sp, a);
+        k_adjoint_step<R, V, MODEL_BGK, DEV><<<grid, block, 0, st>>>(h->sp, a);
       cur ^= 1;
     }
     FLB_CUDA(cudaGetLastError());
@@ -1759,8 +1778,10 @@ int flb_adjoint_backward(flb_lattice* h, double* dJ_dalpha, double* dJ_dtau, dou
     return fail(FLB_ERR_STATE, "dJ/dalpha needs the BRINKMAN model (ALPHA field)");
   cudaStream_t st = as_stream(stream);
   if (h->desc.storage == FLB_STORAGE_FP64)
-    return adjoint_backward_t<double>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
-  return adjoint_backward_t<float>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
+    return adjoint_backward_t<double, double>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
+  if (h->desc.storage == FLB_STORAGE_FP32S)
+    return adjoint_backward_t<dev32, float>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
+  return adjoint_backward_t<float, float>(h, dJ_dalpha, dJ_dtau, dJ_dulid, st);
 }
 
 }  // extern "C"

@@ -35,7 +35,8 @@
 using namespace flb;
 
 namespace flb {
-int report_error(int code, const char* msg);  // flb_api.cu
+int report_error(int code, const char* msg);       // flb_api.cu
+int lattice_storage(const flb_lattice* h);         // flb_api.cu
 }
 
 struct flb_bb {
@@ -373,7 +374,7 @@ int flb_bb_create(flb_lattice* lat, uint8_t cell_flag, uint8_t void_flag, int ki
   bb->kind = kind;
   bb->rho0 = rho0;
   bb->layout = L;
-  bb->storage = L.elem_bytes == 2 ? FLB_STORAGE_FP16S : (L.elem_bytes == 8 ? FLB_STORAGE_FP64 : FLB_STORAGE_FP32);
+  bb->storage = flb::lattice_storage(lat);
   bb->ncells = ncells;
   bb->nlinks = (long long)cell.size();
   if (bb->nlinks > 0) {
@@ -408,11 +409,13 @@ int flb_bb_apply(flb_bb* bb, flb_lattice* lat, void* stream) {
   int rc = flb_get_layout(lat, &L);
   if (rc) return rc;
   if (L.nx != bb->layout.nx || L.ny != bb->layout.ny || L.nz != bb->layout.nz ||
-      L.pitch_x != bb->layout.pitch_x || L.elem_bytes != bb->layout.elem_bytes)
+      L.pitch_x != bb->layout.pitch_x || L.elem_bytes != bb->layout.elem_bytes ||
+      flb::lattice_storage(lat) != bb->storage)
     return report_error(FLB_ERR_INVALID, "flb_bb_apply: lattice differs from the one at creation");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (bb->storage == FLB_STORAGE_FP64) return launch<double, double>(bb, lat, st);
   if (bb->storage == FLB_STORAGE_FP16S) return launch<__half, float>(bb, lat, st);
+  if (bb->storage == FLB_STORAGE_FP32S) return launch<dev32, float>(bb, lat, st);
   return launch<float, float>(bb, lat, st);
 }
 

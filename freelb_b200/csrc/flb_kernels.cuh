@@ -226,6 +226,29 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+// Deterministic FP64 sums: every CTA of a reduction writes its own slot(s) of
+// `partials` (ncomp values per slot, in a fixed order within the CTA) and this
+// kernel adds slots 0..nslots-1 in a fixed order to acc[0..ncomp).  The result
+// does not depend on CTA scheduling, unlike atomics (~1e-14 relative jitter on
+// a sum of millions of terms, enough to swamp a finite difference of it).
+constexpr int RED_SLOTS = 148 * 32;  // the largest grid_1d grid
+static __global__ void __launch_bounds__(256) k_sum_partials(const double* partials,
+                                                             int nslots, int ncomp, double* acc) {
+  __shared__ double red[256];
+  for (int k = 0; k < ncomp; ++k) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nslots; b += 256) s += partials[b * ncomp + k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0;
+      for (int t = 0; t < 256; ++t) v += red[t];
+      acc[k] += v;
+    }
+    __syncthreads();
+  }
+}
+
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_finite(LayoutParams L, const S* pops,
                                                 unsigned long long* acc, StepParams sp) {

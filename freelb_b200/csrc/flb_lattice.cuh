@@ -130,6 +130,27 @@ struct Storage<__half, float> {
   }
 };
 
+// FP32S storage element: d_i = f_i - rho0 w_i held as a float.  A type of its
+// own, so that every kernel templated on the storage knows the stored values
+// are deviations: the step and adjoint kernels work on them directly (a
+// deviation of size ~1e-3 keeps ~5e-11 of absolute resolution, where f_i ~ 0.1
+// in a float keeps ~7e-9), while these load / store forms convert to and from
+// f_i for the readers and writers of populations.
+struct dev32 {
+  float v;
+};
+static_assert(sizeof(dev32) == 4, "FP32S element is one float");
+
+template <>
+struct Storage<dev32, float> {
+  __device__ static __forceinline__ float load(const dev32* p, float shift, float) {
+    return p->v + shift;
+  }
+  __device__ static __forceinline__ void store(dev32* p, float v, float shift, float) {
+    p->v = v - shift;
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Per-cell operators.  f[] holds the 19 populations of one cell in registers.
 

@@ -1,17 +1,18 @@
 // flb_noalloc.cu -- mass/momentum reduction that allocates no memory.
 //
 // flb_reduce_conservation (flb_api.cu) accumulates into a result area the
-// lattice handle allocated with cudaMalloc.  Some callers cannot allocate
-// device memory at the point where they want this check: code that runs while
-// a CUDA stream is being captured into a graph (cudaMalloc is not a stream
-// operation and breaks or is refused during capture), runtimes that hand GPU
-// memory out only through their own pool and forbid direct cudaMalloc, and
-// plugin hosts that call into this library from threads where a driver-level
-// allocation could block on another context's work.  This variant takes the
-// populations and flags as plain device pointers and keeps its scratch -- one
-// partial sum per thread block and the final four sums -- in the file-scope
-// device array below, which every GPU that loads the library holds until the
-// process exits.
+// lattice handle allocated with cudaMalloc.  Some callers cannot let a library
+// allocate device memory: runtimes that hand GPU memory out only through their
+// own caching pool (so that their accounting stays exact and no component
+// triggers the implicit synchronisation a cudaMalloc / cudaFree can cause),
+// and plugin hosts that call into this library from threads where a
+// driver-level allocation could block on another context's work.  This
+// variant takes the populations and flags as plain device pointers and keeps
+// its scratch -- one partial sum per thread block and the final four sums --
+// in the file-scope device array below, which every GPU that loads the library
+// holds until the process exits.  It copies the sums to the caller's host
+// array and synchronises the caller's stream before returning, so it is not a
+// call to make inside a stream capture.
 //
 // Two passes, both deterministic: pass 1 has thread block b reduce the padded
 // cells [b*kCellsPerBlock, (b+1)*kCellsPerBlock) into partial slot b; pass 2
@@ -41,7 +42,11 @@ constexpr int kThreads = 256;
 // 4 sums per partial slot plus the final 4 sums: (4096 + 1) * 4 doubles = 128 KiB.
 __device__ __align__(256) double g_noalloc_scratch[(kMaxPartials + 1) * 4];
 
-// Device address of g_noalloc_scratch, looked up once per device.
+// Device address of g_noalloc_scratch, looked up on the first call on each
+// device (with that device current) and kept for the process.  A
+// cudaDeviceReset on that device unloads the library's device code with this
+// array, after which the kept address is stale: the entry point is not to be
+// called on a device after resetting it.
 std::mutex g_mu;
 void* g_scratch_ptr[64] = {};
 
@@ -85,10 +90,12 @@ __global__ void __launch_bounds__(kThreads)
     if (!decode_cell(L, c, x, y, z)) continue;
     if (!(flags[c] & key)) continue;
     R f[Q];
-    gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
+    gather_stored<S, R>(pops, L.dstride, g, x, y, z, sp, f);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const double v = double(f[i]);
+      // FP16S values come converted; FP32S deviations get their shift in FP64
+      const double v = std::is_same<S, dev32>::value ? double(f[i]) + double(sp.shift[i])
+                                                     : double(f[i]);
       s[0] += v;
       s[1] += cx(i) * v;
       s[2] += cy(i) * v;
@@ -147,8 +154,9 @@ int run(const void* pops, const uint8_t* flags, const flb_layout* lay, double rh
     const double w = i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
     sp.shift[i] = float(rho0 * w);
   }
-  sp.scale = 1024.0f;  // FP16S storage scale of the library
-  sp.inv_scale = 1.0f / 1024.0f;
+  // FP16S storage scale of the library (FP32S deviations are unscaled)
+  sp.scale = std::is_same<S, __half>::value ? 1024.0f : 1.0f;
+  sp.inv_scale = 1.0f / sp.scale;
   const long long total = L.plane * L.nz;
   const int nblocks = int((total + kCellsPerBlock - 1) / kCellsPerBlock);
   k_cons_partials<S, R><<<nblocks, kThreads, 0, st>>>(L, g, static_cast<const S*>(pops), flags,
@@ -178,7 +186,7 @@ int flb_reduce_conservation_noalloc(const void* pops, const uint8_t* flags,
     return report_error(FLB_ERR_INVALID, "flb_reduce_conservation_noalloc: null argument");
   const flb_layout& L = *layout;
   const int elem = storage == FLB_STORAGE_FP16S ? 2 : (storage == FLB_STORAGE_FP64 ? 8 : 4);
-  if (storage < 0 || storage > 2 || L.elem_bytes != elem) {
+  if (storage < 0 || storage > 3 || L.elem_bytes != elem) {
     char m[160];
     std::snprintf(m, sizeof m,
                   "flb_reduce_conservation_noalloc: storage %d does not match %d-byte elements",
@@ -198,7 +206,33 @@ int flb_reduce_conservation_noalloc(const void* pops, const uint8_t* flags,
     return report_error(FLB_ERR_INVALID, m);
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the scratch is the current device's: the stream and the arrays must be on it
+  int dev = 0, sdev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess && st) e = cudaStreamGetDevice(st, &sdev);
+  else sdev = dev;  // the legacy default stream belongs to the current device
+  if (e != cudaSuccess) {
+    char m[160];
+    std::snprintf(m, sizeof m, "flb_reduce_conservation_noalloc: stream device: %s",
+                  cudaGetErrorString(e));
+    return report_error(FLB_ERR_CUDA, m);
+  }
+  for (const void* ptr : {pops, static_cast<const void*>(flags)}) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess ||
+        !(a.type == cudaMemoryTypeManaged || (a.type == cudaMemoryTypeDevice && a.device == dev))) {
+      cudaGetLastError();  // clear a failed query
+      return report_error(FLB_ERR_INVALID,
+                          "flb_reduce_conservation_noalloc: pops and flags must be device memory "
+                          "of the current device");
+    }
+  }
+  if (sdev != dev)
+    return report_error(FLB_ERR_INVALID,
+                        "flb_reduce_conservation_noalloc: stream belongs to another device than "
+                        "the current one");
   if (storage == FLB_STORAGE_FP32) return run<float, float>(pops, flags, layout, rho0, key, out, st);
+  if (storage == FLB_STORAGE_FP32S) return run<dev32, float>(pops, flags, layout, rho0, key, out, st);
   if (storage == FLB_STORAGE_FP64)
     return run<double, double>(pops, flags, layout, rho0, key, out, st);
   return run<__half, float>(pops, flags, layout, rho0, key, out, st);

@@ -26,7 +26,10 @@ namespace flb {
 // the storage conversion of Storage<S, R> (FP16S: shift and scale).
 template <typename S, typename R, int V>
 __device__ __forceinline__ void vload(const S* p, R* out, float shift, float inv_scale) {
-  if constexpr (std::is_same<S, float>::value && V == 4) {
+  if constexpr (std::is_same<S, dev32>::value) {
+    // FP32S: the step and adjoint kernels work on the stored deviations
+    vload<float, R, V>(reinterpret_cast<const float*>(p), out, shift, inv_scale);
+  } else if constexpr (std::is_same<S, float>::value && V == 4) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(p));
     out[0] = v.x;
     out[1] = v.y;
@@ -61,7 +64,9 @@ __device__ __forceinline__ void vload(const S* p, R* out, float shift, float inv
 
 template <typename S, typename R, int V>
 __device__ __forceinline__ void vstore(S* p, const R* in, float shift, float scale) {
-  if constexpr (std::is_same<S, float>::value && V == 4) {
+  if constexpr (std::is_same<S, dev32>::value) {
+    vstore<float, R, V>(reinterpret_cast<float*>(p), in, shift, scale);
+  } else if constexpr (std::is_same<S, float>::value && V == 4) {
     *reinterpret_cast<float4*>(p) = make_float4(in[0], in[1], in[2], in[3]);
   } else if constexpr (std::is_same<S, float>::value && V == 2) {
     *reinterpret_cast<float2*>(p) = make_float2(in[0], in[1]);
@@ -83,6 +88,14 @@ __device__ __forceinline__ void vstore(S* p, const R* in, float shift, float sca
 #pragma unroll
     for (int k = 0; k < V; ++k) Storage<S, R>::store(p + k, in[k], shift, scale);
   }
+}
+
+// One stored value as the step kernels see it (vload's form for one element):
+// FP32S deviations as stored, every other storage through its load form.
+template <typename S, typename R>
+__device__ __forceinline__ R gload(const S* p, float shift, float inv_scale) {
+  if constexpr (std::is_same<S, dev32>::value) return p->v;
+  else return Storage<S, R>::load(p, shift, inv_scale);
 }
 
 // Source of population i for cell (x,y,z) under the reference's streaming:
@@ -171,7 +184,7 @@ __device__ __forceinline__ void gather_chunk(const S* __restrict__ arr, long lon
 #pragma unroll
       for (int i = 1; i < Q; ++i)
         if (SIGN * cx(i) > 0)
-          vals[i][0] = Storage<S, R>::load(
+          vals[i][0] = gload<S, R>(
               arr + i * dstride + wrap_off(g, 0, y, z, -SIGN * cx(i), -SIGN * cy(i), -SIGN * cz(i)),
               shift[i], inv_scale);
     }
@@ -183,7 +196,7 @@ __device__ __forceinline__ void gather_chunk(const S* __restrict__ arr, long lon
 #pragma unroll
           for (int i = 1; i < Q; ++i)
             if (SIGN * cx(i) < 0)
-              vals[i][k] = Storage<S, R>::load(
+              vals[i][k] = gload<S, R>(
                   arr + i * dstride +
                       wrap_off(g, g.nx - 1, y, z, -SIGN * cx(i), -SIGN * cy(i), -SIGN * cz(i)),
                   shift[i], inv_scale);
@@ -196,7 +209,7 @@ __device__ __forceinline__ void gather_chunk(const S* __restrict__ arr, long lon
       const int x = min(x0 + k, g.nx - 1);
 #pragma unroll
       for (int i = 0; i < Q; ++i)
-        vals[i][k] = Storage<S, R>::load(
+        vals[i][k] = gload<S, R>(
             arr + i * dstride + wrap_off(g, x, y, z, -SIGN * cx(i), -SIGN * cy(i), -SIGN * cz(i)),
             shift[i], inv_scale);
     }
@@ -521,10 +534,10 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
   }
 }
 
-// MRT (collision::MRT_Feq_RhoU) on deviations: H <- H - M^-1 S M N.
-__device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q], float omega) {
-  float rho, N[Q];
-  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
+// MRT (collision::MRT_Feq_RhoU) on deviations: H <- H - M^-1 S M N, given the
+// non-equilibrium part N.
+__device__ __forceinline__ void mrt_relax_neq(const StepParams& p, float (&H)[Q], float omega,
+                                              const float (&N)[Q]) {
   float a[9], b[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
@@ -538,12 +551,18 @@ __device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q]
   mrt_relax<float>(H, N[0], a, b, s);
 }
 
-// Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
-// sum c c N / S, the effective rate from it, H <- H - omega_eff N.  Products
-// that meet additions are explicit, as in deviation_neq.
-__device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q], float omega) {
+__device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q], float omega) {
   float rho, N[Q];
   deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
+  mrt_relax_neq(p, H, omega, N);
+}
+
+// Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
+// sum c c N / S, the effective rate from it, H <- H - omega_eff N, given the
+// cell's density and non-equilibrium part.  Products that meet additions are
+// explicit, as in deviation_neq.
+__device__ __forceinline__ void les_relax_neq(const StepParams& p, float (&H)[Q], float omega,
+                                              float rho, const float (&N)[Q]) {
   const float is = p.inv_scale;  // a power of two: the scaling is exact
   const float p0 = is * ((((N[1] + N[2]) + (N[7] + N[8])) + ((N[9] + N[10]) + (N[13] + N[14]))) +
                          (N[15] + N[16]));
@@ -566,6 +585,137 @@ __device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q]
   const float eomega = 1.0f / (rt_mol + rt_tur);
 #pragma unroll
   for (int i = 0; i < Q; ++i) H[i] = fmaf(-eomega, N[i], H[i]);
+}
+
+__device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q], float omega) {
+  float rho, N[Q];
+  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
+  les_relax_neq(p, H, omega, rho, N);
+}
+
+// ---------------------------------------------------------------------------
+// FP32S storage (dev32): d_i = f_i - rho0 w_i in FP32, collided as stored, the
+// FP16S deviation form at full FP32 width with IEEE divisions.
+
+// delta = sum d (= rho - rho0), rho, den = rho + alpha/2 and u = sum c d / den
+// (the weights carry no momentum, so sum c d = sum c f); alpha = 0 gives
+// moment::rhoU, alpha > 0 the forced moments of the Brinkman model.
+__device__ __forceinline__ void dev_moments(const float (&d)[Q], float rho0, float alpha,
+                                            float& delta, float& rho, float& den, float& ux,
+                                            float& uy, float& uz) {
+  float sp[Q], df[Q];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = d[i] + d[i + 1];
+    df[i] = d[i] - d[i + 1];
+  }
+  delta = ((d[0] + sp[1]) + (sp[3] + sp[5])) + ((sp[7] + sp[9]) + (sp[11] + sp[13])) +
+          (sp[15] + sp[17]);
+  const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
+  const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
+  const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
+  rho = rho0 + delta;
+  den = fmaf(0.5f, alpha, rho);
+  ux = mx / den;
+  uy = my / den;
+  uz = mz / den;
+}
+
+// k_i = 3 c_i.u for the first direction of each opposite pair (k of i + 1 is -k_i).
+__device__ __forceinline__ void dev_k(float ux, float uy, float uz, float (&k)[Q]) {
+  const float k1 = __fmul_rn(3.0f, ux), k3 = __fmul_rn(3.0f, uy), k5 = __fmul_rn(3.0f, uz);
+  k[1] = k1;
+  k[3] = k3;
+  k[5] = k5;
+  k[7] = k1 + k3;
+  k[9] = k1 + k5;
+  k[11] = k3 + k5;
+  k[13] = k1 - k3;
+  k[15] = k1 - k5;
+  k[17] = k3 - k5;
+}
+
+// Non-equilibrium part N_i = d_i - E_i with E_i = feq_i - rho0 w_i
+// = w_i (delta + rho g_i), g_i = k_i + k_i^2/2 - 3|u|^2/2 (SecondOrder).
+__device__ __forceinline__ void dev_neq(const float (&d)[Q], float delta, float rho, float ux,
+                                        float uy, float uz, float (&N)[Q]) {
+  const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, __fmul_rn(uz, uz)));
+  float k[Q];
+  dev_k(ux, uy, uz, k);
+  N[0] = fmaf(-(1.0f / 3.0f), fmaf(rho, q, delta), d[0]);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float w = i < 7 ? 1.0f / 18.0f : 1.0f / 36.0f;
+    const float e = fmaf(0.5f * k[i], k[i], q);
+    N[i] = fmaf(-w, fmaf(rho, e + k[i], delta), d[i]);
+    N[i + 1] = fmaf(-w, fmaf(rho, e - k[i], delta), d[i + 1]);
+  }
+}
+
+// collision::BGKForce with the Brinkman drag (bgk_brinkman) on deviations:
+//   d'_i = (1 - omega) d_i + omega w_i (delta + rho g_i) + (1 - omega/2) F_i,
+// F_i = w_i F.(3 (c_i - u) + 9 (c_i.u) c_i) with F = -alpha u, which is
+// -alpha w_i (k_i + k_i^2 - 3|u|^2); the part of both terms odd in c_i is
+// (omega rho - (1 - omega/2) alpha) k_i.
+__device__ __forceinline__ void brinkman_deviation(const StepParams& p, float (&d)[Q],
+                                                   float omega, float alpha) {
+  float delta, rho, den, ux, uy, uz;
+  dev_moments(d, p.rho0, alpha, delta, rho, den, ux, uy, uz);
+  const float u2 = fmaf(ux, ux, fmaf(uy, uy, __fmul_rn(uz, uz)));
+  const float q = -1.5f * u2, t = -3.0f * u2;
+  const float c1 = 1.0f - omega;
+  const float fa = __fmul_rn(1.0f - 0.5f * omega, alpha);
+  const float odd = fmaf(omega, rho, -fa);
+  float k[Q];
+  dev_k(ux, uy, uz, k);
+  d[0] = fmaf(c1, d[0], (1.0f / 3.0f) * fmaf(omega, fmaf(rho, q, delta), -__fmul_rn(fa, t)));
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float w = i < 7 ? 1.0f / 18.0f : 1.0f / 36.0f;
+    const float e = fmaf(0.5f * k[i], k[i], q);
+    const float h = fmaf(k[i], k[i], t);
+    const float ge = fmaf(omega, fmaf(rho, e, delta), -__fmul_rn(fa, h));
+    const float go = __fmul_rn(odd, k[i]);
+    d[i] = fmaf(c1, d[i], w * (ge + go));
+    d[i + 1] = fmaf(c1, d[i + 1], w * (ge - go));
+  }
+}
+
+// One FP32S cell by its op.  Bounce-back and the moving wall act on the
+// deviations as they act on f (w_i = w_opp(i), and the wall term is additive);
+// the field-velocity BGK goes through f.
+template <int MODEL>
+__device__ __forceinline__ void collide_dev32(const StepParams& p, int op, float (&d)[Q],
+                                              long long cell, float omega) {
+  if (op == OP_NONE) return;
+  if (op == OP_BB || op == OP_MBB) {
+    apply_wall_op<float>(p, op, d, cell, omega);
+    return;
+  }
+  if (op == OP_BULK) {
+    if constexpr (MODEL == MODEL_BRINKMAN) {
+      brinkman_deviation(p, d, omega, static_cast<const float*>(p.alpha)[cell]);
+    } else {
+      float delta, rho, den, ux, uy, uz, N[Q];
+      dev_moments(d, p.rho0, 0.0f, delta, rho, den, ux, uy, uz);
+      dev_neq(d, delta, rho, ux, uy, uz, N);
+      if constexpr (MODEL == MODEL_MRT) {
+        mrt_relax_neq(p, d, omega, N);
+      } else if constexpr (MODEL == MODEL_LES) {
+        les_relax_neq(p, d, omega, rho, N);
+      } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) d[i] = fmaf(-omega, N[i], d[i]);
+      }
+    }
+    return;
+  }
+  float f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[i] = d[i] + p.shift[i];
+  apply_wall_op<float>(p, op, f, cell, omega);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) d[i] = f[i] - p.shift[i];
 }
 
 // One cell: bulk BGK through the pair form (both lanes the same cell), bulk
@@ -778,7 +928,21 @@ __device__ __forceinline__ void pull_chunk(const StepParams& p, const Geom& g, R
   const long long cell0 = g.base + (long long)y * g.pitch + (long long)z * g.plane + x0;
   uint8_t fl[V];
   load_flags<V>(p.flags + cell0, fl);
-  collide_chunk<R, MODEL, V>(p, g, omega, vals, fl, cell0, nvalid);
+  if constexpr (std::is_same<S, dev32>::value) {
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      if (k < nvalid) {
+        float d[Q];
+#pragma unroll
+        for (int i = 0; i < Q; ++i) d[i] = vals[i][k];
+        collide_dev32<MODEL>(p, select_op(p, fl[k]), d, cell0 + k, omega);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) vals[i][k] = d[i];
+      }
+    }
+  } else {
+    collide_chunk<R, MODEL, V>(p, g, omega, vals, fl, cell0, nvalid);
+  }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
     R v[V];
@@ -819,7 +983,7 @@ struct PullBounds {
   static constexpr int min_ctas =
       std::is_same<S, double>::value                          ? 1
       : std::is_same<S, __half>::value && MODEL == MODEL_BGK ? 2
-      : std::is_same<S, float>::value && V == 4               ? 2
+      : (std::is_same<S, float>::value || std::is_same<S, dev32>::value) && V == 4 ? 2
                                                               : 3;
 };
 
@@ -885,8 +1049,11 @@ __global__ void k_unstream_in(LayoutParams L, Geom g, const H* stage, S* pops_i,
        c += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
-    Storage<S, R>::store(pops_i + wrap_src(g, x, y, z, i),
-                         R(stage[((long long)z * L.ny + y) * L.nx + x]), shift, scale);
+    const H v = stage[((long long)z * L.ny + y) * L.nx + x];
+    if constexpr (std::is_same<S, dev32>::value)  // the deviation in the host precision
+      pops_i[wrap_src(g, x, y, z, i)].v = float(v - H(shift));
+    else
+      Storage<S, R>::store(pops_i + wrap_src(g, x, y, z, i), R(v), shift, scale);
   }
 }
 
@@ -898,8 +1065,12 @@ __global__ void k_stream_out(LayoutParams L, Geom g, H* stage, const S* pops_i, 
        c += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
-    stage[((long long)z * L.ny + y) * L.nx + x] =
-        H(Storage<S, R>::load(pops_i + wrap_src(g, x, y, z, i), shift, inv_scale));
+    H v;
+    if constexpr (std::is_same<S, dev32>::value)
+      v = H(pops_i[wrap_src(g, x, y, z, i)].v) + H(shift);
+    else
+      v = H(Storage<S, R>::load(pops_i + wrap_src(g, x, y, z, i), shift, inv_scale));
+    stage[((long long)z * L.ny + y) * L.nx + x] = v;
   }
 }
 
@@ -913,6 +1084,36 @@ __device__ __forceinline__ void gather_R(const S* pops, long long dstride, const
                                sp.inv_scale);
 }
 
+// the same as stored values (FP32S: the deviations, unconverted)
+template <typename S, typename R>
+__device__ __forceinline__ void gather_stored(const S* pops, long long dstride, const Geom& g,
+                                              int x, int y, int z, const StepParams& sp, R* v) {
+#pragma unroll
+  for (int i = 0; i < Q; ++i)
+    v[i] = gload<S, R>(pops + i * dstride + wrap_src(g, x, y, z, i), sp.shift[i], sp.inv_scale);
+}
+
+// rho and u of cell (x,y,z) (forced moments where a porosity field is given)
+template <typename S, typename R>
+__device__ __forceinline__ void cell_rho_u(const S* pops, long long dstride, const Geom& g, int x,
+                                           int y, int z, const StepParams& sp, R alpha, R& r,
+                                           R& ux, R& uy, R& uz) {
+  R f[Q];
+  if constexpr (std::is_same<S, dev32>::value) {
+    gather_stored<S, R>(pops, dstride, g, x, y, z, sp, f);
+    R delta, den;
+    dev_moments(f, sp.rho0, alpha, delta, r, den, ux, uy, uz);
+  } else {
+    gather_R<S, R>(pops, dstride, g, x, y, z, sp, f);
+    if (sp.alpha) {
+      R den;
+      forced_moments<R>(f, alpha, r, den, ux, uy, uz);
+    } else {
+      rho_u<R>(f, r, ux, uy, uz);
+    }
+  }
+}
+
 template <typename S, typename R>
 __global__ void k_rhou_pull(LayoutParams L, Geom g, const S* pops, const uint8_t* flags,
                             uint8_t key, R* rho, R* vel, StepParams sp) {
@@ -922,14 +1123,10 @@ __global__ void k_rhou_pull(LayoutParams L, Geom g, const S* pops, const uint8_t
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
     if (!(flags[g.base + c] & key)) continue;
-    R f[Q], r, ux, uy, uz;
-    gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
-    if (sp.alpha) {
-      R den;
-      forced_moments<R>(f, static_cast<const R*>(sp.alpha)[g.base + c], r, den, ux, uy, uz);
-    } else {
-      rho_u<R>(f, r, ux, uy, uz);
-    }
+    R r, ux, uy, uz;
+    cell_rho_u<S, R>(pops, L.dstride, g, x, y, z, sp,
+                     sp.alpha ? static_cast<const R*>(sp.alpha)[g.base + c] : R(0), r, ux, uy,
+                     uz);
     rho[g.base + c] = r;
     vel[g.base + c] = ux;
     vel[g.base + c + L.dstride] = uy;
@@ -937,10 +1134,12 @@ __global__ void k_rhou_pull(LayoutParams L, Geom g, const S* pops, const uint8_t
   }
 }
 
+// Mass and momentum sums of one block: CTA b writes partials[4b .. 4b+3]
+// (k_sum_partials adds them in a fixed order).
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_conservation_pull(LayoutParams L, Geom g, const S* pops,
                                                            const uint8_t* flags, uint8_t key,
-                                                           double* acc, StepParams sp) {
+                                                           double* partials, StepParams sp) {
   double s[4] = {0, 0, 0, 0};
   const long long total = L.plane * L.nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
@@ -949,10 +1148,12 @@ __global__ void __launch_bounds__(256) k_conservation_pull(LayoutParams L, Geom 
     if (!decode_cell(L, c, x, y, z)) continue;
     if (!(flags[g.base + c] & key)) continue;
     R f[Q];
-    gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
+    gather_stored<S, R>(pops, L.dstride, g, x, y, z, sp, f);
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
-      const double v = double(f[i]);
+      // FP16S values come converted; FP32S deviations get their shift in FP64
+      const double v = std::is_same<S, dev32>::value ? double(f[i]) + double(sp.shift[i])
+                                                     : double(f[i]);
       s[0] += v;
       s[1] += cx(i) * v;
       s[2] += cy(i) * v;
@@ -970,7 +1171,7 @@ __global__ void __launch_bounds__(256) k_conservation_pull(LayoutParams L, Geom 
   if (threadIdx.x < 4) {
     double v = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
-    atomicAdd(acc + threadIdx.x, v);
+    partials[blockIdx.x * 4 + threadIdx.x] = v;
   }
 }
 
@@ -986,9 +1187,14 @@ __global__ void __launch_bounds__(256) k_tolerance_pull(LayoutParams L, Geom g, 
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
     if (!(flags[g.base + c] & key)) continue;
-    R f[Q], r, ux, uy, uz;
-    gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
-    rho_u<R>(f, r, ux, uy, uz);
+    R r, ux, uy, uz;
+    if constexpr (std::is_same<S, dev32>::value) {
+      cell_rho_u<S, R>(pops, L.dstride, g, x, y, z, sp, R(0), r, ux, uy, uz);
+    } else {
+      R f[Q];
+      gather_R<S, R>(pops, L.dstride, g, x, y, z, sp, f);
+      rho_u<R>(f, r, ux, uy, uz);
+    }
     const double u[3] = {double(ux), double(uy), double(uz)};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {

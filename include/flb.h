@@ -54,6 +54,7 @@ extern "C" {
 #define FLB_STORAGE_FP32 0  /* f_i as float */
 #define FLB_STORAGE_FP16S 1 /* f_i - rho0*w_i as half, float arithmetic */
 #define FLB_STORAGE_FP64 2  /* f_i as double, double arithmetic */
+#define FLB_STORAGE_FP32S 3 /* f_i - rho0*w_i as float, float arithmetic on the deviations */
 
 /* bulk collision model (the policy bound to FLB_OP_BULK) */
 #define FLB_MODEL_BGK 0 /* collision::BGK<moment::rhoU, equilibrium::SecondOrder> */
@@ -227,7 +228,8 @@ FLB_API int flb_step(flb_lattice* lat, int nsteps, void* stream);
 FLB_API int flb_compute_rhou(flb_lattice* lat, uint8_t key, void* stream);
 
 /* FP64 sums over cells whose flag shares a bit with `key`:
- * out[0] = sum rho, out[1..3] = sum rho*u (mass and momentum). */
+ * out[0] = sum rho, out[1..3] = sum rho*u (mass and momentum).  Summed in a
+ * fixed order: the same state gives the same bits on every call. */
 FLB_API int flb_reduce_conservation(flb_lattice* lat, uint8_t key, double out[4], void* stream);
 
 /* Steady-state check: max |u - u_prev| over cells matching `key` since the
@@ -261,22 +263,27 @@ FLB_API int flb_device_pointers(flb_lattice* lat, void** pops, void** flags, voi
  * triggers the implicit synchronisation a cudaMalloc/cudaFree can cause), or a
  * latency-bound loop that must not wait on an allocation, cannot let this
  * library call cudaMalloc behind its back.  Here the caller passes its own
- * device pointers -- populations `pops` and `flags` laid out as `layout`
- * describes (flb_get_layout / flb_device_pointers give both for a handle),
- * `storage` (FLB_STORAGE_*) and `rho0` (the FP16S shift density) -- and a host
- * array `out` for the four sums; the function allocates nothing.
+ * device pointers -- populations `pops` and `flags` of ONE block laid out as
+ * `layout` describes (flb_get_layout / flb_device_pointers give both for a
+ * single-block handle; on a multi-block handle they describe block 0 only),
+ * `storage` (FLB_STORAGE_*) and `rho0` (the FP16S / FP32S shift density) --
+ * and a host array `out` for the four sums; the function allocates nothing.
+ * `pops`, `flags` and `stream` must belong to the current device
+ * (FLB_ERR_INVALID otherwise).
  *
  * Its scratch is a fixed device array inside the library: 128 KiB, held on
  * every GPU that loads the library until the process exits.  That bounds the
  * lattice to 268,435,456 padded cells (layout->plane * layout->nz); larger
  * layouts are rejected with FLB_ERR_INVALID.  The first call on a device looks
- * up the array's device address for that device, so make that first call
- * before capturing any stream.  Every call on a device uses the same scratch
- * and it keeps the previous call's contents; nothing in it needs to start at
- * zero (each call writes every slot it reads), but calls whose work overlaps
- * on the GPU (different streams, different host threads) race on it and must
- * be serialised by the caller.  `stream` orders the work and is synchronised
- * before returning. */
+ * up the array's device address for that device and keeps it for the process,
+ * so do not call it on a device after a cudaDeviceReset of that device.  Every
+ * call on a device uses the same scratch and it keeps the previous call's
+ * contents; nothing in it needs to start at zero (each call writes every slot
+ * it reads), but calls whose work overlaps on the GPU (different streams,
+ * different host threads) race on it and must be serialised by the caller.
+ * `stream` orders the work; the call copies the sums to `out` and
+ * synchronises `stream` before returning, so it cannot be called while
+ * `stream` is being captured into a CUDA graph. */
 FLB_API int flb_reduce_conservation_noalloc(const void* pops, const uint8_t* flags,
                                             const flb_layout* layout, int storage, double rho0,
                                             uint8_t key, double out[4], void* stream);
@@ -323,12 +330,15 @@ FLB_API int flb_step_graph(flb_lattice* lat, int nsteps, void* stream);
 
 /* Objective J = sum over bulk cells of |u|^2 at the current state, with the
  * forced moment u = sum c f / (rho + alpha/2) (alpha = 0 without a porosity
- * field), reduced in FP64. */
+ * field), reduced in FP64 in a fixed order (the same state gives the same
+ * bits, so central differences of J are not swamped by summation order). */
 FLB_API int flb_objective_u2(flb_lattice* lat, double* J, void* stream);
 
 /* Discrete adjoint of the step (no reference counterpart: the reference has no
- * differentiation).  Single-block handles, FP32 or FP64 storage, ops none /
- * bulk (BGK, BRINKMAN or MRT) / bounce-back / moving wall.
+ * differentiation).  Single-block handles, FP32, FP32S or FP64 storage, ops
+ * none / bulk (BGK, BRINKMAN or MRT) / bounce-back / moving wall.  FP32S keeps
+ * the forward trajectory within ~1e-7 of an FP64 run where FP32 storage of f
+ * drifts by ~1e-5, which is what a per-cell gradient needs.
  * flb_adjoint_forward advances nsteps from the current state, keeping a copy of
  * the state every `checkpoint_every` steps, and returns J at the end.
  * flb_adjoint_backward returns dJ/dalpha (per cell, N doubles in reference
@@ -338,7 +348,8 @@ FLB_API int flb_objective_u2(flb_lattice* lat, double* J, void* stream);
  * device memory of the pair (ceil(nsteps / checkpoint_every) checkpoints and
  * checkpoint_every - 1 recompute slots of the population size, two adjoint
  * arrays, the dJ/dalpha array), so flb_adjoint_backward allocates nothing;
- * flb_adjoint_release frees it. */
+ * a later flb_adjoint_forward with the same nsteps / checkpoint_every reuses
+ * them, and flb_adjoint_release frees them. */
 FLB_API int flb_adjoint_forward(flb_lattice* lat, int nsteps, int checkpoint_every, double* J,
                                 void* stream);
 FLB_API int flb_adjoint_backward(flb_lattice* lat, double* dJ_dalpha, double* dJ_dtau,

@@ -37,7 +37,7 @@ extern "C" {
 typedef struct flb_bb flb_bb;
 
 /* Build a manager from the lattice's current flags (BlockFixedBoundary::Setup,
- * basic_boundary.h:213-262).  rho0 is the FP16S shift density of the lattice. */
+ * basic_boundary.h:213-262).  rho0 is the FP16S / FP32S shift density of the lattice. */
 FLB_API int flb_bb_create(flb_lattice* lat, uint8_t cell_flag, uint8_t void_flag, int kind,
                           double rho0, flb_bb** out);
 /* Boundary cells and (cell, direction) links of the manager. */

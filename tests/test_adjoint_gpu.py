@@ -3,7 +3,10 @@ against central finite differences of FP64 forward runs.
 
 The objective is J = sum over bulk cells of |u|^2 at step T with
 u = sum c f / (rho + alpha/2); the parameters are the per-cell porosity alpha,
-tau and the lid speed.  Tolerances are stated per test.
+tau and the lid speed.  Tolerances are stated per test.  The per-cell bar is
+1e-4 relative for FP64 and FP32S storage (FP32 deviations f - rho0 w); FP32
+storage of f itself carries a trajectory error of ~1e-5 that leaves cells with
+small gradients above 1e-4, so it is held to 1e-3.
 """
 import numpy as np
 import pytest
@@ -21,11 +24,13 @@ def brinkman_cavity(ni, tau, ulid, alpha, storage):
     return lat
 
 
-@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5), ("fp32s", 1e-6)])
 def test_brinkman_forward_matches_oracle(gpu_ok, storage, tol):
+    """FP32S is held against the FP64 oracle: it stores deviations, so its
+    trajectory follows FP64, not the FP32 rounding of f."""
     ni, tau, steps = 14, 0.56, 60
     a = O.porosity(ni, 3)
-    dt = np.float64 if storage == "fp64" else np.float32
+    dt = np.float32 if storage == "fp32" else np.float64
     lat = brinkman_cavity(ni, tau, 0.1, a, storage)
     lat.step(steps)
     ref = O.cavity(ni, model="brinkman", tau=tau, ulid=0.1, dtype=dt, alpha=a)
@@ -42,7 +47,7 @@ def fd_objective(ni, tau, ulid, alpha, steps, storage="fp64"):
     return j
 
 
-@pytest.mark.parametrize("storage,tol", [("fp64", 1e-6), ("fp32", 1e-3)])
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-6), ("fp32s", 1e-4), ("fp32", 1e-3)])
 def test_adjoint_gradients_match_central_differences(gpu_ok, storage, tol):
     """dJ/dalpha on seeded cells, dJ/dtau and dJ/du_lid against FP64 central
     differences (h = 1e-4).  Checkpoints every 25 steps over 70 steps exercise
@@ -54,7 +59,7 @@ def test_adjoint_gradients_match_central_differences(gpu_ok, storage, tol):
     J = lat.adjoint_forward(steps, every)
     g_alpha, g_tau, g_ulid = lat.adjoint_backward()
     J64 = fd_objective(ni, tau, ulid, a, steps)
-    assert abs(J - J64) / J64 < (1e-12 if storage == "fp64" else 1e-4)
+    assert abs(J - J64) / J64 < {"fp64": 1e-12, "fp32s": 1e-6, "fp32": 1e-4}[storage]
     h = 1e-4
     flags = F.cavity_flags(ni)
     fluid = np.flatnonzero(flags == 2)
@@ -80,9 +85,10 @@ def test_adjoint_gradients_match_central_differences(gpu_ok, storage, tol):
     assert abs(g_ulid - fd_u_h) <= 1e-4 * abs(fd_u_h)
     # the lattice keeps the forward end state
     ref = O.cavity(ni, model="brinkman", tau=tau, ulid=ulid,
-                   dtype=np.float64 if storage == "fp64" else np.float32, alpha=a)
+                   dtype=np.float32 if storage == "fp32" else np.float64, alpha=a)
     ref.step(steps)
-    assert rel_maxnorm(lat.download_pops(), ref.pops) < (1e-12 if storage == "fp64" else 1e-5)
+    assert rel_maxnorm(lat.download_pops(), ref.pops) < {"fp64": 1e-12, "fp32s": 1e-6,
+                                                         "fp32": 1e-5}[storage]
     # non-bulk cells carry no porosity gradient
     assert np.all(g_alpha.reshape(n, n, n)[0] == 0)
 
@@ -109,7 +115,7 @@ def test_adjoint_plain_bgk_tau_and_lid(gpu_ok):
     assert abs(g_ulid - fd_u) <= 1e-6 * abs(fd_u), (g_ulid, fd_u)
 
 
-@pytest.mark.parametrize("storage,tol", [("fp64", 1e-6), ("fp32", 2e-3)])
+@pytest.mark.parametrize("storage,tol", [("fp64", 1e-6), ("fp32s", 1e-4), ("fp32", 2e-3)])
 def test_adjoint_mrt_tau_and_lid(gpu_ok, storage, tol):
     """MRT (Gram-Schmidt D3Q19 basis, shear rates 1/tau, others 1.2): the
     transposed collision Jacobian gives dJ/dtau and dJ/du_lid matching FP64
@@ -124,7 +130,7 @@ def test_adjoint_mrt_tau_and_lid(gpu_ok, storage, tol):
         m.step(steps)
         return m.objective_u2()
 
-    assert abs(J - Jf(tau, ulid)) / J < (1e-12 if storage == "fp64" else 1e-4)
+    assert abs(J - Jf(tau, ulid)) / J < {"fp64": 1e-12, "fp32s": 1e-6, "fp32": 1e-4}[storage]
     h = 1e-4
     d1 = (Jf(tau + h, ulid) - Jf(tau - h, ulid)) / (2 * h)
     d2 = (Jf(tau + h / 2, ulid) - Jf(tau - h / 2, ulid)) / h
@@ -174,3 +180,16 @@ def test_adjoint_matches_reference_solver_finite_differences(gpu_ok):
     d2 = (j_ref(a, tau + h / 2) - j_ref(a, tau - h / 2)) / h
     fd_tau = (4 * d2 - d1) / 3
     assert abs(g_tau - fd_tau) <= 1e-6 * abs(fd_tau), (g_tau, fd_tau)
+
+
+@pytest.mark.parametrize("storage", ["fp64", "fp32s", "fp32"])
+def test_objective_and_conservation_sums_are_deterministic(gpu_ok, storage):
+    """J and the mass / momentum sums are FP64 reductions in a fixed order: the
+    same state gives the same bits on every call (a finite difference of J at
+    h = 1e-4 needs J to 1e-15 relative, below the jitter of atomic sums)."""
+    lat = brinkman_cavity(40, 0.56, 0.1, O.porosity(40, 4), storage)
+    lat.step(30)
+    js = {lat.objective_u2() for _ in range(5)}
+    assert len(js) == 1, js
+    sums = [lat.conservation(key=2) for _ in range(5)]
+    assert all(np.array_equal(s, sums[0]) for s in sums)

@@ -21,7 +21,8 @@ from freelb_b200 import _capi as C
 
 pytestmark = pytest.mark.gpu
 
-STORAGE = {"fp32": C.STORAGE_FP32, "fp16s": C.STORAGE_FP16S, "fp64": C.STORAGE_FP64}
+STORAGE = {"fp32": C.STORAGE_FP32, "fp16s": C.STORAGE_FP16S, "fp64": C.STORAGE_FP64,
+           "fp32s": C.STORAGE_FP32S}
 
 
 def noalloc_sums(lat, key):
@@ -43,7 +44,7 @@ def assert_same_sums(got, want):
     assert np.all(np.abs(got - want) <= 1e-12 * scale), (got, want)
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp64"])
+@pytest.mark.parametrize("storage", ["fp32", "fp16s", "fp64", "fp32s"])
 def test_noalloc_matches_allocating_reduction_on_consecutive_calls(gpu_ok, storage):
     lat = F.cavity(40, tau=0.55, ulid=0.1, storage=storage)
     lat.step(25)
@@ -84,3 +85,19 @@ def test_noalloc_rejects_layouts_beyond_its_scratch(gpu_ok):
                                              2, out, None)
     assert rc == -1    # FLB_ERR_INVALID
     assert "268435456" in lib.flb_last_error().decode()
+
+
+def test_noalloc_rejects_host_memory(gpu_ok):
+    """Arrays that are not device memory of the current device are refused
+    before any GPU work (the scratch and the kernels are the current device's)."""
+    lat = F.cavity(8, storage="fp32")
+    lib = C.load()
+    host = np.zeros(19 * lat.layout().dir_stride, dtype=np.float32)
+    flags = ctypes.c_void_p()
+    C.call("flb_device_pointers", lat._h, None, ctypes.byref(flags), None, None)
+    out = (ctypes.c_double * 4)()
+    rc = lib.flb_reduce_conservation_noalloc(ctypes.c_void_p(host.ctypes.data), flags,
+                                             ctypes.byref(lat.layout()), C.STORAGE_FP32, 1.0,
+                                             2, out, None)
+    assert rc == -1    # FLB_ERR_INVALID
+    assert "device memory" in lib.flb_last_error().decode()
