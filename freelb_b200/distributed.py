@@ -22,7 +22,7 @@ import numpy as np
 from . import _capi as C
 from . import Lattice, _stream
 
-ELEM_BYTES = {"fp32": 4, "fp16s": 2, "fp64": 8}
+ELEM_BYTES = {"fp32": 4, "fp16s": 2, "fp64": 8, "fp32s": 4}
 HALO_MODES = {"normal": C.HALO_NORMAL, "full": C.HALO_FULL}
 
 
@@ -63,7 +63,8 @@ def plan(blocks, owners, rank, halo_mode="normal"):
 def nccl_exchange(send, recv, group=None):
     """Move the per-peer buffers: one batch of point-to-point sends and receives
     (every rank posts its sends and receives in peer order, so the batch pairs
-    up on both sides)."""
+    up on both sides).  The operations are ordered after the work already on
+    torch's current stream, and that stream waits for them (req.wait())."""
     import torch.distributed as dist
     ops = []
     for peer in sorted(set(send) | set(recv)):
@@ -74,6 +75,19 @@ def nccl_exchange(send, recv, group=None):
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
+
+
+def host_exchange(send, recv, group=None):
+    """The same exchange through host memory, for process groups whose backend
+    moves only CPU tensors (gloo): device buffers are copied out on torch's
+    current stream (which synchronises it), sent and received as one batch, and
+    copied back on that stream."""
+    import torch.distributed as dist
+    hsend = {p: b.cpu() for p, b in send.items() if b.numel()}
+    hrecv = {p: b.new_empty(b.shape, device="cpu") for p, b in recv.items() if b.numel()}
+    nccl_exchange(hsend, hrecv, group)
+    for p, b in hrecv.items():
+        recv[p].copy_(b)
 
 
 class RankLattice:
@@ -121,15 +135,34 @@ class RankLattice:
 
     def step(self, n=1, stream=None, exchange=None, group=None):
         """n steps: stream-collide plus local halo (flb_step), then pack, the
-        exchange (default: NCCL through torch.distributed) and unpack."""
-        for _ in range(n):
-            self.lat.step(1, stream)
-            self.pack(stream)
-            if exchange is None:
-                nccl_exchange(self.send, self.recv, group)
-            else:
-                exchange(self)
-            self.unpack(stream)
+        exchange and unpack.  `exchange`: None or "nccl" (NCCL through
+        torch.distributed), "host" (through host memory, for gloo), or a
+        callable taking this RankLattice.  `stream` (a torch.cuda.Stream, a raw
+        cudaStream_t as int, or None for torch's current stream) orders all of
+        it: the exchange runs with that stream as torch's current stream, so
+        the library's pack / unpack kernels and the transfers between them are
+        ordered on one stream."""
+        import torch
+        if stream is None:
+            ts = torch.cuda.current_stream()
+        elif isinstance(stream, int):
+            ts = torch.cuda.ExternalStream(stream)
+        else:
+            ts = stream
+        move = None
+        if not callable(exchange):
+            move = {None: nccl_exchange, "nccl": nccl_exchange, "host": host_exchange}.get(exchange)
+            if move is None:
+                raise ValueError(f"unknown exchange {exchange!r}")
+        with torch.cuda.stream(ts):
+            for _ in range(n):
+                self.lat.step(1, ts)
+                self.pack(ts)
+                if move is not None:
+                    move(self.send, self.recv, group)
+                else:
+                    exchange(self)
+                self.unpack(ts)
 
     def close(self):
         if getattr(self, "_ex", None) and self._ex.value:

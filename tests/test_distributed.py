@@ -176,3 +176,70 @@ def test_exchange_rejects_a_handle_that_does_not_match(gpu_ok):
     with pytest.raises(F.FlbError):
         rl.pack()
     rl.close()
+
+
+def _gpu_rank(rank, world, port, q, storage, steps, own_stream):
+    """One process of a two-slab cavity on cuda:0: its RankLattice, stepped with
+    the host transport over gloo, returns its blocks' populations."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        torch.cuda.set_device(0)
+        blocks = D.slabs(12, world)
+        owners = list(range(world))
+        ni = 12
+        n = ni + 2
+        flags = F.cavity_flags(ni)
+        real = np.float64 if storage == "fp64" else np.float32
+        u = np.zeros((n ** 3, 3), dtype=real)
+        u[flags == 8, 0] = real(0.1)
+        rl = D.RankLattice(blocks, owners, rank, 0.55, storage=storage)
+        for k, b in enumerate(rl.local):
+            rl.lat.upload_flags(G.slice_block(flags, n, b), block=k)
+            rl.lat.upload_field("u", G.slice_block(u, n, b, comps=3), block=k)
+        stream = torch.cuda.Stream() if own_stream else None
+        rl.step(steps, stream=stream, exchange="host")
+        torch.cuda.synchronize()
+        q.put((rank, [rl.lat.download_pops(block=k) for k in range(len(rl.local))]))
+        rl.close()
+    except Exception as e:  # reported by the parent
+        q.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["fp32", "fp16s"])
+def test_two_processes_on_one_gpu_equal_single_block(gpu_ok, storage):
+    """Two processes (gloo ranks) on cuda:0, each holding the RankLattice of one
+    z-slab of a 12^3 cavity, exchange their packed halo buffers through host
+    memory every step; rank 1 orders its work on a stream of its own.  The
+    fluid cells of both slabs equal the single-block run bit for bit.  No
+    kernel of one process waits on the other's: each step's buffers cross on
+    the host between the two processes' launches."""
+    world, steps = 2, 20
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_rank, args=(r, world, port, q, storage, steps, r == 1))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    ni = 12
+    n = ni + 2
+    one = F.cavity(ni, tau=0.55, storage=storage)
+    one.step(steps)
+    P = one.download_pops().reshape(19, n, n, n)
+    flags = F.cavity_flags(ni)
+    for r, b in enumerate(D.slabs(ni, world)):
+        assert not isinstance(res[r], str), res[r]
+        pb = res[r][0].reshape(19, b["nz"], b["ny"], b["nx"])
+        fb = G.slice_block(flags, n, b).reshape(b["nz"], b["ny"], b["nx"])
+        ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
+        assert np.array_equal(pb[:, fb == 2], ps[:, fb == 2]), r
