@@ -92,6 +92,56 @@ def build_examples(force: bool = False) -> str:
     return EXAMPLE_BIN
 
 
+# The reference's own programs, their sources untouched, built against the
+# host classes (only the include path differs): kind -> (source under the
+# reference root, output name, compiler, extra flags).  The cavity3d example is
+# built for both of its FLOAT_TYPE settings (its Makefile uses double).
+REF_PROGRAMS = {
+    "cpu": ("benchmarks/cavity3d/cavity3d.cpp", "ref_cavity3d", "g++", []),
+    "cu": ("benchmarks/cavity3d_cu/cavity3d.cu", "ref_cavity3d_cu", "nvcc", []),
+    "example": ("examples/cavity3d/cavity3d.cpp", "ref_example_cavity3d", "g++",
+                ["-DFLOAT_TYPE=double"]),
+    "example_f32": ("examples/cavity3d/cavity3d.cpp", "ref_example_cavity3d_f32", "g++",
+                    ["-DFLOAT_TYPE=float"]),
+}
+
+
+def ref_program_path(kind: str) -> str:
+    return os.path.join(HERE, "cpp", "_build", REF_PROGRAMS[kind][1])
+
+
+def build_reference_program(kind: str, ref_root: str, force: bool = False) -> str:
+    """Compile one of the reference's programs (read in place under ref_root)
+    against the host classes and libflb_b200.so; returns the executable."""
+    rel, _, cc, extra = REF_PROGRAMS[kind]
+    src = os.path.join(ref_root, rel)
+    out = ref_program_path(kind)
+    deps = [src, os.path.join(HERE, "cpp", "freelb.h"), LIB]
+    if not force and not _stale(out, deps):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    inc = os.path.join(HERE, "cpp")
+    if cc == "nvcc":
+        cmd = [nvcc(), "-std=c++17", *ARCH, "-I" + inc, *extra, src, "-L" + HERE, "-lflb_b200",
+               "-Xlinker", "-rpath,$ORIGIN/../..", "-o", out]
+    else:
+        cmd = ["g++", "-std=c++17", "-O1", "-I" + inc, *extra, src, "-L" + HERE, "-lflb_b200",
+               "-Wl,-rpath,$ORIGIN/../..", "-o", out]
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    res = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if res.returncode != 0:
+        raise RuntimeError(f"{cc} failed on {rel}:\n" + res.stdout + res.stderr[-4000:])
+    return out
+
+
+def build_reference_programs(ref_root: str, force: bool = False) -> dict:
+    """All of REF_PROGRAMS whose source exists under ref_root."""
+    return {k: build_reference_program(k, ref_root, force) for k, v in REF_PROGRAMS.items()
+            if os.path.exists(os.path.join(ref_root, v[0]))}
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
     print(build_examples(force="--force" in sys.argv))
