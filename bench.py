@@ -35,7 +35,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 Q = 19
-BYTES_PER_POP = {"fp32": 4, "fp16s": 2, "fp64": 8}
+BYTES_PER_POP = {"fp32": 4, "fp16s": 2, "fp64": 8, "fp32s": 4}
+CPU_BASELINE_STEPS = 20   # ~8 s of the reference's OpenMP path at 512^3 on 16 host cores
+MRT_PARITY_STEPS = 20     # the reference's generic MRT runs ~3 s per 256^3 step on 14 cores
 
 
 def algo_bytes_per_cell(storage: str) -> int:
@@ -146,7 +148,7 @@ def run_reference_arm(args, rank, world):
     ni = args.ni
     cells = (ni + 2) ** 3
     steps = max(1, min(args.steps, 20))
-    warm = min(args.warmup, 1)
+    warm = args.warmup
     r = reference_cpu(ni, steps, warm)
     base = {"impl": "reference", "metric": "D3Q19 cavity GLUPs (stored cells)", "unit": "GLUPs",
             "n_gpus": args.gpus, "higher_is_better": True}
@@ -170,6 +172,18 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------------------- our arm
+
+def compact(v, digits=4):
+    """Floats rounded to `digits` significant digits, recursively (keeps the
+    JSON line short enough to be read whole from a log tail)."""
+    if isinstance(v, float):
+        return float(f"{v:.{digits}g}") if np.isfinite(v) else v
+    if isinstance(v, dict):
+        return {k: compact(x, digits) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [compact(x, digits) for x in v]
+    return v
+
 
 def max_over_ranks(torch, dist, value, device):
     """Largest value over all ranks (the job time of independent replicas)."""
@@ -214,28 +228,104 @@ def timed_cavity(F, torch, stream, ni, steps, warmup, storage="fp32", model="bgk
     return t.ms, launch, lat
 
 
-def accuracy_block(F, ni, steps):
+def accuracy_block(F, ni, steps, keep_bgk_fp32=False):
     """Relative L2 error of u after `steps` steps against an FP64 run of the same
-    kernel, per model and storage (C2 accuracy report)."""
-    out = {}
+    kernel, per model and storage (C2 accuracy report).  LES also reports the
+    spread of two FP64 runs whose initial populations differ by 1e-7 (relative,
+    seeded): the flow's own sensitivity, beside which the storage errors read.
+    With keep_bgk_fp32 the FP32 BGK populations (reference order) are returned
+    for the parity check against the reference's own FP32 run."""
+    out, kept = {}, None
     for model, tau in (("bgk", 0.53), ("mrt", 0.53), ("les", 3 * 0.1 * ni / 10000 + 0.5)):
         us = {}
-        for storage in ("fp64", "fp32", "fp16s"):
+        for storage in ("fp64", "fp32", "fp32s", "fp16s"):
             lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model)
             lat.step(steps)
             _, u = lat.rhou(key=2, dtype=np.float64)
             us[storage] = u
+            if keep_bgk_fp32 and model == "bgk" and storage == "fp32":
+                kept = (lat.download_pops(), lat.download_field("rho"), u.astype(np.float32))
             lat.close()
         ref = np.linalg.norm(us["fp64"])
-        out[model] = {"tau": tau,
-                      "fp32_rel_l2_u": float(np.linalg.norm(us["fp32"] - us["fp64"]) / ref),
-                      "fp16s_rel_l2_u": float(np.linalg.norm(us["fp16s"] - us["fp64"]) / ref)}
-    return {"config": f"{ni}^3 cavity, {steps} steps, u_lid=0.1 (LES: Cs=0.1, Re=10000)",
-            "models": out}
+        out[model] = {"tau": tau, **{f"{s}_rel_l2_u": float(np.linalg.norm(us[s] - us["fp64"]) / ref)
+                                     for s in ("fp32", "fp32s", "fp16s")}}
+        if model == "les":
+            n = ni + 2
+            lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
+            w = np.repeat(np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12), n ** 3)
+            xi = np.random.default_rng(123).standard_normal(19 * n ** 3)
+            lat.upload_pops(w * (1.0 + 1e-7 * xi))
+            lat.step(steps)
+            _, u = lat.rhou(key=2, dtype=np.float64)
+            lat.close()
+            out[model]["fp64_perturbed_1e-7_rel_l2_u"] = float(np.linalg.norm(u - us["fp64"]) / ref)
+        del us
+    res = {"config": f"{ni}^3 cavity, {steps} steps, u_lid=0.1 (LES: Cs=0.1, Re=10000)",
+           "models": out}
+    return (res, kept) if keep_bgk_fp32 else res
+
+
+class ReferenceParity:
+    """The reference's own FP32 CPU path (oracle/_ref) on the 256^3 cavity, run in
+    a background process while the GPU sections run: BGK for the full 2000 steps
+    of the accuracy run, MRT (26x slower per cell in the reference's generic
+    MRT_Feq_RhoU) for a bounded number of steps.  compare() checks the GPU's FP32
+    results against its dumps (relative max-norm over every cell)."""
+
+    def __init__(self, ni, bgk_steps, mrt_steps):
+        import tempfile
+        import threading
+        from oracle import oracle as O
+        self.O = O
+        self.ni, self.bgk_steps, self.mrt_steps = ni, bgk_steps, mrt_steps
+        self.dir = tempfile.TemporaryDirectory(prefix="flb_refpar_")
+        self.res, self.err = {}, None
+        self.threads = max(1, (os.cpu_count() or 2) - 2)  # leave the GPU driver thread a core
+        if O.ref_binary(np.float32) is None:
+            self.err = "reference harness oracle/_ref not built"
+            self.t = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _run(self):
+        try:
+            for model, steps in (("bgk", self.bgk_steps), ("mrt", self.mrt_steps)):
+                d = os.path.join(self.dir.name, model)
+                os.makedirs(d)
+                t0 = time.time()
+                r = self.O.run_reference(model, self.ni, 0.53, 0.1, steps, 0, threads=self.threads,
+                                         outdir=d)
+                self.res[model] = {"dump": d, "seconds": time.time() - t0, "mlups": r["mlups"]}
+        except Exception as e:  # reported in the bench line
+            self.err = f"{type(e).__name__}: {e}"
+
+    def compare(self, model, pops, rho, u):
+        if self.t is not None:
+            self.t.join()
+        if model not in self.res:
+            return {"unavailable": self.err or "not run"}
+        r = self.O.load_dump(self.res[model]["dump"], np.float32)
+        flags = r["flags"]
+        fl = flags == 2
+        out = {"steps": self.bgk_steps if model == "bgk" else self.mrt_steps,
+               "ref_threads": self.threads, "ref_seconds": self.res[model]["seconds"],
+               "pops": self.O.rel_maxnorm(pops, r["pops"]),
+               "rho_fluid": self.O.rel_maxnorm(rho[fl], r["rho"][fl]),
+               "u_fluid": self.O.rel_maxnorm(u.reshape(-1, 3)[fl], r["u"].reshape(-1, 3)[fl])}
+        return out
+
+    def close(self):
+        if self.t is not None:
+            self.t.join()
+        self.dir.cleanup()
 
 
 def blocks_block(F, torch, stream, ni, steps, seed=0):
-    """Uneven-block 256^3 cavity with device halos vs the single-block run."""
+    """Uneven-block 256^3 cavity with device halos, timed, then checked against
+    the single-block run of the same number of steps: flags equal, and the
+    populations of every fluid cell (max relative difference; bit-for-bit by
+    construction)."""
     from freelb_b200 import geometry as G
     blocks = G.uneven_blocks(ni, edges=(32, 48, 64, 96), seed=seed)
     n = ni + 2
@@ -246,14 +336,32 @@ def blocks_block(F, torch, stream, ni, steps, seed=0):
     for k, b in enumerate(blocks):
         lat.upload_flags(G.slice_block(flags, n, b), block=k)
         lat.upload_field("u", G.slice_block(u, n, b, comps=3), block=k)
-    launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
+    launch, _, taken = lat.autotune(trial_steps=2, stream=stream)
     with DeviceTimer(torch, stream) as t:
         lat.step(steps, stream)
     stored = sum(b["nx"] * b["ny"] * b["nz"] for b in blocks)
     res = {"blocks": len(blocks), "stored_cells": stored, "halo_records": lat.halo_count(),
            "launch": launch, "glups_stored": stored * steps / (t.ms / 1e3) / 1e9,
            "glups_domain": n ** 3 * steps / (t.ms / 1e3) / 1e9}
+    one = F.cavity(ni, tau=0.53, ulid=0.1)
+    one.step(taken + steps, stream)
+    P = one.download_pops().reshape(19, n, n, n)
+    one.close()
+    flags_ok, diff, cells = True, 0.0, 0
+    pmax = float(np.max(np.abs(P)))
+    for k, b in enumerate(blocks):
+        fb = lat.download_flags(block=k).reshape(b["nz"], b["ny"], b["nx"])
+        fg = G.slice_block(flags, n, b).reshape(b["nz"], b["ny"], b["nx"])
+        flags_ok &= bool(np.array_equal(fb, fg))
+        pb = lat.download_pops(block=k).reshape(19, b["nz"], b["ny"], b["nx"])
+        ps = P[:, b["oz"]:b["oz"] + b["nz"], b["oy"]:b["oy"] + b["ny"], b["ox"]:b["ox"] + b["nx"]]
+        m = fg == 2
+        d = np.abs(pb[:, m].astype(np.float64) - ps[:, m])
+        diff = max(diff, float(d.max()) if d.size else 0.0)
+        cells += int(m.sum())
     lat.close()
+    res.update({"check_steps": taken + steps, "flags_equal": flags_ok, "fluid_cells": cells,
+                "fluid_pops_max_rel_diff": diff / pmax})
     return res
 
 
@@ -261,7 +369,7 @@ def ensemble_block(F, torch, stream, steps, count=128, seed=0):
     """128 independent cavities (n ~ U{32..128}, Re ~ logU[100, 3000],
     tau = 3 u_lid n / Re + 0.5) in one multi-block handle (tile work table,
     autotuned, CUDA-graph stepping) against one handle per cavity stepped one
-    after another."""
+    after another, for FP32 and FP16S storage."""
     rng = np.random.default_rng(seed)
     sizes = [int(v) for v in rng.integers(32, 129, size=count)]
     res_ = np.exp(rng.uniform(np.log(100.0), np.log(3000.0), size=count))
@@ -284,26 +392,30 @@ def ensemble_block(F, torch, stream, steps, count=128, seed=0):
             lat.step(steps, stream, graph=True)
         out[storage] = {"batched_glups": cells * steps / (t.ms / 1e3) / 1e9, "launch": launch}
         lat.close()
-    # one-at-a-time: a handle per cavity, each stepped `steps` times in turn
-    lats = [F.cavity(n, tau=t, ulid=0.1) for n, t in zip(sizes, taus)]
-    for lat in lats:
-        lat.step(1, stream)
-    with DeviceTimer(torch, stream) as t:
-        for _ in range(steps):
-            for lat in lats:
-                lat.step(1, stream)
-    out["fp32"]["sequential_glups"] = cells * steps / (t.ms / 1e3) / 1e9
-    for lat in lats:
-        lat.close()
+        # one-at-a-time: a handle per cavity, each stepped `steps` times in turn
+        lats = [F.cavity(n, tau=t, ulid=0.1, storage=storage) for n, t in zip(sizes, taus)]
+        for one in lats:
+            one.step(1, stream)
+        with DeviceTimer(torch, stream) as t:
+            for _ in range(steps):
+                for one in lats:
+                    one.step(1, stream)
+        out[storage]["sequential_glups"] = cells * steps / (t.ms / 1e3) / 1e9
+        for one in lats:
+            one.close()
     return out
 
 
 def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, seed=0):
     """128^3 cavity, Re = 500 (tau = 3*0.1*128/500 + 0.5), porosity alpha ~
     U[0, 0.05]; J = sum |u|^2 at T = 2000; checkpoints every 100 steps; FP32
-    forward and adjoint, FP64 gradient accumulation.  Reports the adjoint-to-
-    forward time ratio and the gradient's relative error against FP64 central
-    differences (h = 1e-4) on 32 seeded fluid cells, on tau and on u_lid."""
+    forward and adjoint, FP64 gradient accumulation.  Two FP32 storage forms:
+    FP32S (deviations f - w, the form the gradient bar is met with) and FP32
+    storage of f.  Per form: the backward-to-forward time ratio, the full
+    gradient (checkpointed forward + backward) against a plain forward, and the
+    gradient's relative error against FP64 central differences (h = 1e-4) on 32
+    seeded fluid cells, on tau and on u_lid.  The timed pair is the second one
+    on the handle (the first allocates the checkpoints)."""
     tau = 3 * 0.1 * ni / 500 + 0.5
     n = ni + 2
     alpha = np.random.default_rng(seed).uniform(0.0, 0.05, size=n ** 3)
@@ -312,18 +424,6 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, 
         lat = F.cavity(ni, tau=t, ulid=ulid, storage=storage, model="brinkman")
         lat.upload_field("alpha", a.astype(lat.real))
         return lat
-
-    lat = lattice("fp32")
-    lat.step(2, stream)
-    with DeviceTimer(torch, stream) as tf:
-        lat.step(steps, stream)
-    lat.close()
-    lat = lattice("fp32")
-    with DeviceTimer(torch, stream) as tfc:
-        lat.adjoint_forward(steps, every, stream)
-    with DeviceTimer(torch, stream) as tb:
-        g_alpha, g_tau, g_ulid = lat.adjoint_backward(stream=stream)
-    lat.close()
 
     def J(a=alpha, t=tau, ulid=0.1):
         m = lattice("fp64", a, t, ulid)
@@ -336,31 +436,48 @@ def adjoint_block(F, torch, stream, ni=128, steps=2000, every=100, fd_cells=32, 
     flags = F.cavity_flags(ni)
     fluid = np.flatnonzero(flags == 2)
     cells = np.random.default_rng(seed + 1).choice(fluid, size=fd_cells, replace=False)
-    errs, fds = [], []
+    fds = []
     for c in cells:
         ap, am = alpha.copy(), alpha.copy()
         ap[c] += h
         am[c] -= h
-        fd = (J(ap) - J(am)) / (2 * h)
-        fds.append(fd)
-        errs.append(abs(g_alpha[c] - fd) / abs(fd))
+        fds.append((J(ap) - J(am)) / (2 * h))
     fds = np.array(fds)
-    norm_err = float(np.linalg.norm(g_alpha[cells] - fds) / np.linalg.norm(fds))
     fd_tau = (J(t=tau + h) - J(t=tau - h)) / (2 * h)
     fd_ulid = (J(ulid=0.1 + h) - J(ulid=0.1 - h)) / (2 * h)
-    return {"config": f"{ni}^3, T={steps}, checkpoints every {every}, tau={tau:.4f}",
+    out = {"config": f"{ni}^3, T={steps}, checkpoints every {every}, tau={tau:.4f}",
+           "fd_cells": int(fd_cells), "dJ_dtau_fd": fd_tau, "dJ_dulid_fd": fd_ulid}
+    for storage in ("fp32s", "fp32"):
+        lat = lattice(storage)
+        lat.step(2, stream)
+        with DeviceTimer(torch, stream) as tf:
+            lat.step(steps, stream)
+        lat.close()
+        lat = lattice(storage)
+        lat.adjoint_forward(steps, every, stream)
+        lat.adjoint_backward(stream=stream)
+        lat.init_equilibrium(1.0, stream)  # back to the initial state, buffers kept
+        with DeviceTimer(torch, stream) as tfc:
+            lat.adjoint_forward(steps, every, stream)
+        with DeviceTimer(torch, stream) as tb:
+            g_alpha, g_tau, g_ulid = lat.adjoint_backward(stream=stream)
+        lat.close()
+        errs = np.abs(g_alpha[cells] - fds) / np.abs(fds)
+        out[storage] = {
             "forward_ms_per_step": tf.ms / steps,
             "forward_with_checkpoints_ms_per_step": tfc.ms / steps,
             "backward_ms_per_step": tb.ms / steps,
             "adjoint_to_forward_ratio": tb.ms / tf.ms,
+            "full_gradient_to_forward_ratio": (tfc.ms + tb.ms) / tf.ms,
             "dJ_dtau": g_tau, "dJ_dulid": g_ulid,
-            "fd_cells": int(fd_cells),
             "fd_rel_err_alpha_max": float(np.max(errs)),
             "fd_rel_err_alpha_median": float(np.median(errs)),
-            "fd_rel_err_alpha_normwise": norm_err,
-            "fd_rel_err_alpha": [float(e) for e in errs],
+            "fd_rel_err_alpha_normwise": float(np.linalg.norm(g_alpha[cells] - fds) /
+                                               np.linalg.norm(fds)),
+            "fd_cells_above_1e-4": int(np.sum(errs > 1e-4)),
             "fd_rel_err_tau": float(abs(g_tau - fd_tau) / abs(fd_tau)),
             "fd_rel_err_ulid": float(abs(g_ulid - fd_ulid) / abs(fd_ulid))}
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -437,14 +554,23 @@ def run_ours(args, rank, world, local_rank):
     h2d = flags.nbytes + u0.nbytes
     d2h = out_rho.nbytes + out_u.nbytes
 
+    # the reference's CPU path on the same cavity (host cores, bounded sample),
+    # before any background CPU work starts
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu(ni, CPU_BASELINE_STEPS, 0)
+
     extras = {}
     if world == 1 and not args.quick:
+        par_ni = 256
+        refpar = ReferenceParity(par_ni, 2000, MRT_PARITY_STEPS) if not args.no_parity else None
         # other models and storages on the same 512^3 cavity
         variants = {}
         les_tau = 3 * 0.1 * ni / 10000 + 0.5
         for storage, model, tau in (("fp16s", "bgk", 0.53), ("fp32", "mrt", 0.53),
                                     ("fp16s", "mrt", 0.53), ("fp32", "les", les_tau),
-                                    ("fp16s", "les", les_tau), ("fp64", "bgk", 0.53)):
+                                    ("fp16s", "les", les_tau), ("fp64", "bgk", 0.53),
+                                    ("fp32s", "bgk", 0.53)):
             ms, lch, vl = timed_cavity(F, torch, stream, ni, args.steps, 2, storage, model,
                                        tau=tau)
             bad = vl.nonfinite()
@@ -452,18 +578,26 @@ def run_ours(args, rank, world, local_rank):
             b = algo_bytes_per_cell(storage)
             ach = cells * b / (ms / args.steps / 1e3) / 1e9
             variants[f"{model}_{storage}"] = {
-                "glups": cells * args.steps / (ms / 1e3) / 1e9, "ms_per_step": ms / args.steps,
-                "launch": lch, "achieved_gbs": ach, "frac": ach / measured_peaks()[0],
-                "algorithmic_bytes_per_cell": b, "tau": tau, "nonfinite": bad}
+                "glups": cells * args.steps / (ms / 1e3) / 1e9, "frac": ach / measured_peaks()[0],
+                "launch": lch, "nonfinite": bad}
         extras["variants"] = variants
-        extras["accuracy"] = accuracy_block(F, args.accuracy_ni, 2000)
+        acc = accuracy_block(F, args.accuracy_ni, 2000, keep_bgk_fp32=args.accuracy_ni == par_ni)
+        extras["accuracy"], kept = acc if isinstance(acc, tuple) else (acc, None)
         extras["blocks_256"] = blocks_block(F, torch, stream, 256, args.steps)
         extras["ensemble_128"] = ensemble_block(F, torch, stream, args.steps)
         extras["adjoint_128"] = adjoint_block(F, torch, stream)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = reference_cpu(ni, 3, 0)
+        if refpar is not None:
+            par = {}
+            if kept is not None:
+                par["bgk_fp32"] = refpar.compare("bgk", *kept)
+            del kept
+            m = F.cavity(par_ni, tau=0.53, ulid=0.1, storage="fp32", model="mrt")
+            m.step(MRT_PARITY_STEPS, stream)
+            rho, u = m.rhou(key=2)
+            par["mrt_fp32"] = refpar.compare("mrt", m.download_pops(), rho, u)
+            m.close()
+            refpar.close()
+            extras["parity_256_vs_reference"] = par
 
     if dist:
         dist.barrier()
@@ -488,7 +622,8 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {"fp32": "f32", "fp16s": "f32 (fp16 storage)", "fp64": "f64"}[args.storage],
+        "dtype": {"fp32": "f32", "fp16s": "f32 (fp16 storage)", "fp64": "f64",
+                  "fp32s": "f32 (fp32 deviation storage)"}[args.storage],
         "data": "synthetic",
         "config": {"workload": f"lid-driven cavity {ni}^3 D3Q19 BGK tau=0.53 u_lid=0.1",
                    "stored_cells": cells, "storage": args.storage, "per_gpu": "independent cavity",
@@ -508,13 +643,13 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "nonfinite": bad32,
     }
-    line.update(extras)
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["mlups"] / 1000.0, "unit": "GLUPs",
                                 "cores": cpu["threads"], "kind": "reference",
-                                "sample": f"3 timed steps of the {ni}^3 cavity on the reference "
-                                          f"FreeLB OpenMP path ({cpu['binary']})"}
-    print(json.dumps(line))
+                                "sample": f"{CPU_BASELINE_STEPS} timed steps of the {ni}^3 cavity "
+                                          f"on the reference FreeLB OpenMP path ({cpu['binary']})"}
+    line.update(extras)
+    print(json.dumps(compact(line)))
 
 
 def main():
@@ -525,13 +660,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ni", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "fp64"],
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "fp64", "fp32s"],
                     help="population storage of the headline run (profiling)")
     ap.add_argument("--launch", default=None,
                     help="tile_y,ctas_per_sm,cells_per_thread for the headline run instead of "
                          "the autotuner (profiling)")
     ap.add_argument("--accuracy-ni", type=int, default=256,
                     help="cavity size of the FP64-referenced velocity error report (256 or 512)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the 256^3 parity runs of the reference's CPU path (background)")
     ap.add_argument("--quick", action="store_true",
                     help="headline and e2e only (no variants / accuracy / blocks / ensemble / "
                          "adjoint blocks)")
