@@ -249,16 +249,22 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False):
         ref = np.linalg.norm(us["fp64"])
         out[model] = {"tau": tau, **{f"{s}_rel_l2_u": float(np.linalg.norm(us[s] - us["fp64"]) / ref)
                                      for s in ("fp32", "fp32s", "fp16s")}}
+        if keep_bgk_fp32 and model == "bgk":
+            kept = kept + (us["fp64"],)
         if model == "les":
+            # FP64 runs from initial populations perturbed by eps (relative,
+            # seeded): 1e-7, and 2^-12, the rounding of one FP16 store
             n = ni + 2
-            lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
             w = np.repeat(np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12), n ** 3)
             xi = np.random.default_rng(123).standard_normal(19 * n ** 3)
-            lat.upload_pops(w * (1.0 + 1e-7 * xi))
-            lat.step(steps)
-            _, u = lat.rhou(key=2, dtype=np.float64)
-            lat.close()
-            out[model]["fp64_perturbed_1e-7_rel_l2_u"] = float(np.linalg.norm(u - us["fp64"]) / ref)
+            for name, eps in (("1e-7", 1e-7), ("2^-12", 2.0 ** -12)):
+                lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
+                lat.upload_pops(w * (1.0 + eps * xi))
+                lat.step(steps)
+                _, u = lat.rhou(key=2, dtype=np.float64)
+                lat.close()
+                out[model][f"fp64_perturbed_{name}_rel_l2_u"] = float(
+                    np.linalg.norm(u - us["fp64"]) / ref)
         del us
     res = {"config": f"{ni}^3 cavity, {steps} steps, u_lid=0.1 (LES: Cs=0.1, Re=10000)",
            "models": out}
@@ -300,7 +306,11 @@ class ReferenceParity:
         except Exception as e:  # reported in the bench line
             self.err = f"{type(e).__name__}: {e}"
 
-    def compare(self, model, pops, rho, u):
+    def compare(self, model, pops, rho, u, u64=None):
+        """Relative max-norms (populations on every cell, rho and u on fluid
+        cells) of the GPU's FP32 run against the reference's; with u64 (the
+        GPU's FP64 run, which equals the reference's FP64 path), the relative
+        L2 distance of u from it for both FP32 runs."""
         if self.t is not None:
             self.t.join()
         if model not in self.res:
@@ -308,11 +318,18 @@ class ReferenceParity:
         r = self.O.load_dump(self.res[model]["dump"], np.float32)
         flags = r["flags"]
         fl = flags == 2
+        ru = r["u"].reshape(-1, 3)[fl].astype(np.float64)
         out = {"steps": self.bgk_steps if model == "bgk" else self.mrt_steps,
                "ref_threads": self.threads, "ref_seconds": self.res[model]["seconds"],
                "pops": self.O.rel_maxnorm(pops, r["pops"]),
                "rho_fluid": self.O.rel_maxnorm(rho[fl], r["rho"][fl]),
-               "u_fluid": self.O.rel_maxnorm(u.reshape(-1, 3)[fl], r["u"].reshape(-1, 3)[fl])}
+               "u_fluid": self.O.rel_maxnorm(u.reshape(-1, 3)[fl], ru)}
+        if u64 is not None:
+            v = u64.reshape(-1, 3)[fl]
+            nv = np.linalg.norm(v)
+            out["ref_fp32_vs_fp64_rel_l2_u"] = float(np.linalg.norm(ru - v) / nv)
+            out["ours_fp32_vs_fp64_rel_l2_u"] = float(
+                np.linalg.norm(u.reshape(-1, 3)[fl].astype(np.float64) - v) / nv)
         return out
 
     def close(self):

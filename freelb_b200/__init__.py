@@ -186,6 +186,15 @@ class Lattice:
     def set_launch(self, tile_y=8, ctas_per_sm=0, cells_per_thread=0):
         C.call("flb_set_launch", self._h, int(tile_y), int(ctas_per_sm), int(cells_per_thread))
 
+    def set_wait_limit(self, seconds):
+        """Bound of one device-side wait of the bulk-copy kernel (seconds)."""
+        C.call("flb_set_wait_limit", self._h, float(seconds))
+
+    def device_status(self, stream=None):
+        """Raise FlbError(FLB_ERR_TIMEOUT) if a device-side wait gave up since
+        the last check (and clear it)."""
+        C.call("flb_device_status", self._h, _stream(stream))
+
     def get_launch(self):
         """(tile_y, ctas_per_sm, cells_per_thread)."""
         a, b, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -90,6 +90,9 @@ SIGNATURES = {
     "flb_download_field_block": [_P, _I, _I, _P, _I, _P],
     "flb_set_launch": [_P, _I, _I, _I],
     "flb_get_launch": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "flb_set_wait_limit": [_P, ctypes.c_double],
+    "flb_device_status": [_P, _P],
+    "flb_test_withhold_tile": [_P, ctypes.c_longlong],
     "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)],
     "flb_step_graph": [_P, _I, _P],

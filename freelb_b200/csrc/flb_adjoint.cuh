@@ -312,13 +312,15 @@ __global__ void __launch_bounds__(256) k_adjoint_step(const StepParams p, const 
 // Objective J = sum_{bulk cells} |u|^2 at the current state, its seed
 // lambda_T = dJ/dR_T and the direct term dJ/dalpha = -|u|^2 / (rho + alpha/2).
 // With seed == false only J is accumulated (finite-difference evaluations).
-// CTA b writes its share of J to partials[b]; k_sum_partials adds them in a
-// fixed order, so J is the same bits on every evaluation of the same state.
+// Compensated (double-double) sums: CTA b writes its share of J as the pair
+// partials[2b], partials[2b + 1]; k_sum_partials_dd adds them in a fixed order,
+// so J is the same bits on every evaluation of the same state and carries no
+// summation error that a central difference of J would divide by 2h.
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const S* pops,
                                                    StepParams sp, R* lam, double* galpha,
                                                    double* partials, bool seed) {
-  double jsum = 0;
+  dd jsum;
   const long long total = L.plane * L.nz;
   const R* alpha = static_cast<const R*>(sp.alpha);
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const
       forced_moments(f, al, rho, den, ux, uy, uz);
     }
     const R u2 = ux * ux + uy * uy + uz * uz;
-    jsum += double(u2);
+    jsum.add(double(u2));
     if (seed) {
 #pragma unroll
       for (int j = 0; j < Q; ++j)
@@ -353,14 +355,23 @@ __global__ void __launch_bounds__(256) k_objective(LayoutParams L, Geom g, const
       if (galpha) galpha[c] = -double(u2) / double(den);
     }
   }
-  jsum = warp_sum(jsum);
-  __shared__ double red[8];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = jsum;
+  jsum = warp_sum_dd(jsum);
+  __shared__ double red[2][8];
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = jsum.hi;
+    red[1][threadIdx.x >> 5] = jsum.lo;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double v = 0;
-    for (int w = 0; w < int(blockDim.x >> 5); ++w) v += red[w];
-    partials[blockIdx.x] = v;
+    dd v;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+      dd x;
+      x.hi = red[0][w];
+      x.lo = red[1][w];
+      v.add(x);
+    }
+    partials[2 * blockIdx.x] = v.hi;
+    partials[2 * blockIdx.x + 1] = v.lo;
   }
 }
 

@@ -25,9 +25,11 @@
 #include "../../include/flb_vtk.h"
 #include "flb_adjoint.cuh"
 #include "flb_pipe.cuh"
+#include "flb_tma.cuh"
 #include "flb_vtk.cuh"
 
 using namespace flb;
+static_assert(TMA_TIMEOUT == FLB_ERR_TIMEOUT, "device status code");
 
 namespace {
 
@@ -112,8 +114,12 @@ struct flb_lattice {
   bool halo32 = false;
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
-  int ctas_per_sm = 0;  // -1: the FP16S async-copy pipeline (k_pull_pipe)
+  int ctas_per_sm = 0;  // -1: the FP16S async-copy pipeline (k_pull_pipe);
+                        // -2 / -3: the FP16S bulk-copy kernel with 3 / 5 stages (k_pull_tma)
   int pipe_ctas = 0;    // resident k_pull_pipe CTAs per SM (0 = not yet queried)
+  bool tma_ready = false;  // k_pull_tma shared-memory attributes set
+  double wait_s = 2.0;     // bound of one device-side wait (k_pull_tma)
+  long long withhold = -1; // failure-detection test hook (flb_test_withhold_tile)
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -133,6 +139,10 @@ struct flb_lattice {
 namespace flb {
 int lattice_storage(const flb_lattice* h) { return h->desc.storage; }
 }  // namespace flb
+
+// Device status word of a handle: the last slot of its 64-byte result area
+// (zeroed at creation; the reductions use the first five slots).
+inline int* status_word(flb_lattice* h) { return reinterpret_cast<int*>(h->acc + 7); }
 
 namespace {
 
@@ -468,6 +478,34 @@ int pipe_prepare(flb_lattice* h) {
   }
 }
 
+// The bulk-copy kernel covers single-block FP16S handles with 32-bit offsets
+// whose rows start on 16-byte boundaries and end at most 16 halves before the
+// next row (BGK, MRT, LES) at 4 cells per thread.
+bool tma_supported(const flb_lattice* h) {
+  const LayoutParams& L = h->blocks[0].L;
+  return h->desc.storage == FLB_STORAGE_FP16S && h->mode < 0 && h->sp.idx32 &&
+         h->desc.model != FLB_MODEL_BRINKMAN && L.pitch % 8 == 0 && L.pitch - L.nx <= 16;
+}
+
+template <int MODEL, int NS>
+int tma_attr() {
+  FLB_CUDA(cudaFuncSetAttribute(k_pull_tma<MODEL, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tma_smem_bytes<NS>()));
+  return FLB_OK;
+}
+
+int tma_prepare(flb_lattice* h) {
+  if (h->tma_ready) return FLB_OK;
+  FLB_TRY((tma_attr<MODEL_BGK, 3>()));
+  FLB_TRY((tma_attr<MODEL_BGK, 5>()));
+  FLB_TRY((tma_attr<MODEL_MRT, 3>()));
+  FLB_TRY((tma_attr<MODEL_MRT, 5>()));
+  FLB_TRY((tma_attr<MODEL_LES, 3>()));
+  FLB_TRY((tma_attr<MODEL_LES, 5>()));
+  h->tma_ready = true;
+  return FLB_OK;
+}
+
 // Round-up division constants for q / d, q < 2^31 (Granlund & Montgomery,
 // "Division by invariant integers using multiplication", PLDI 1994, Thm 4.2):
 // s = ceil(log2 d), m = ceil(2^(31+s) / d) < 2^32, q / d = (q m >> 32) >> (s - 1).
@@ -513,6 +551,24 @@ StepParams block_half_params(const flb_lattice* h) {
 
 template <typename S, typename R, int MODEL, int V>
 void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
+  if constexpr (std::is_same<S, __half>::value && V == 4 && MODEL != MODEL_BRINKMAN) {
+    if (h->ctas_per_sm <= -2) {  // flb_set_launch admits it only where tma_supported
+      const HostBlock& b = h->blocks[0];
+      TmaParams tp{};
+      tp.ntiles = (b.padded() + TMA_CELLS - 1) / TMA_CELLS;
+      tp.status = status_word(h);
+      tp.wait_ns = (unsigned long long)(h->wait_s * 1e9);
+      tp.drain_ns = std::max(tp.wait_ns, 1000000000ULL);
+      tp.withhold = h->withhold;
+      const unsigned g = unsigned(std::max(1LL, std::min(tp.ntiles, (long long)h->sm_count)));
+      const StepParams sp = half_step_params<TMA_V>(h);  // 2-cell chunks
+      if (h->ctas_per_sm == -2)
+        k_pull_tma<MODEL, 3><<<g, TMA_THREADS, tma_smem_bytes<3>(), st>>>(sp, tp);
+      else
+        k_pull_tma<MODEL, 5><<<g, TMA_THREADS, tma_smem_bytes<5>(), st>>>(sp, tp);
+      return;
+    }
+  }
   if constexpr (std::is_same<S, __half>::value && V == PIPE_V && MODEL != MODEL_BRINKMAN) {
     if (h->ctas_per_sm < 0) {  // flb_set_launch admits -1 only where pipe_supported
       const HostBlock& b = h->blocks[0];
@@ -1356,10 +1412,17 @@ int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_th
                 cells_per_thread);
   if (tile_y != 1 && tile_y != 2 && tile_y != 4 && tile_y != 8)
     return fail(FLB_ERR_INVALID, "tile_y %d not in {1,2,4,8}", tile_y);
-  if (ctas_per_sm < -1 || ctas_per_sm > 32)
-    return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [-1, 32]", ctas_per_sm);
+  if (ctas_per_sm < -3 || ctas_per_sm > 32)
+    return fail(FLB_ERR_INVALID, "ctas_per_sm %d outside [-3, 32]", ctas_per_sm);
   const int v = cells_per_thread ? cells_per_thread : default_vec(h->desc.storage);
-  if (ctas_per_sm < 0) {
+  if (ctas_per_sm <= -2) {
+    if (!tma_supported(h))
+      return fail(FLB_ERR_UNSUPPORTED,
+                  "ctas_per_sm -2 / -3 (bulk-copy kernel) needs a single-block FP16S handle "
+                  "with 16-byte aligned rows");
+    if (v != 4) return fail(FLB_ERR_INVALID, "ctas_per_sm -2 / -3 runs 4 cells per thread");
+    FLB_TRY(tma_prepare(h));
+  } else if (ctas_per_sm < 0) {
     if (!pipe_supported(h))
       return fail(FLB_ERR_UNSUPPORTED,
                   "ctas_per_sm -1 (async-copy pipeline) needs a single-block FP16S handle");
@@ -1372,6 +1435,36 @@ int flb_set_launch(flb_lattice* h, int tile_y, int ctas_per_sm, int cells_per_th
   h->ctas_per_sm = ctas_per_sm;
   h->vec = v;
   return FLB_OK;
+}
+
+int flb_set_wait_limit(flb_lattice* h, double seconds) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (!(seconds >= 0.0 && seconds <= 60.0))
+    return fail(FLB_ERR_INVALID, "wait limit %g s outside [0, 60]", seconds);
+  h->wait_s = seconds;
+  drop_graphs(h);  // the captured launches carry the old limit
+  return FLB_OK;
+}
+
+int flb_test_withhold_tile(flb_lattice* h, long long tile) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (tile < -1) return fail(FLB_ERR_INVALID, "tile %lld < -1", tile);
+  h->withhold = tile;
+  drop_graphs(h);
+  return FLB_OK;
+}
+
+int flb_device_status(flb_lattice* h, void* stream) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  cudaStream_t st = as_stream(stream);
+  int v = 0;
+  FLB_CUDA(cudaMemcpyAsync(&v, status_word(h), sizeof v, cudaMemcpyDeviceToHost, st));
+  FLB_CUDA(cudaStreamSynchronize(st));
+  if (v == 0) return FLB_OK;
+  FLB_CUDA(cudaMemsetAsync(status_word(h), 0, sizeof v, st));
+  FLB_CUDA(cudaStreamSynchronize(st));
+  return fail(v, "a device-side wait gave up (status %d): the steps since the last check "
+                 "are incomplete", v);
 }
 
 int flb_get_launch(const flb_lattice* h, int* tile_y, int* ctas_per_sm, int* cells_per_thread) {
@@ -1440,6 +1533,27 @@ int flb_autotune(flb_lattice* h, int trial_steps, void* stream, int* tile_y, int
         best_ty = 4;
         best_c = -1;
         best_v = PIPE_V;
+      }
+    }
+  }
+  for (int ns = -2; !rc && ns >= -3 && tma_supported(h); --ns) {  // the bulk-copy kernel
+    rc = flb_set_launch(h, 4, ns, 4);
+    if (!rc) rc = step_any(h, 1, st);
+    if (!rc) {
+      cudaEventRecord(e0, st);
+      rc = step_any(h, trial_steps, st);
+      cudaEventRecord(e1, st);
+    }
+    if (!rc) {
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      taken += trial_steps + 1;
+      if (ms < best) {
+        best = ms;
+        best_ty = 4;
+        best_c = ns;
+        best_v = 4;
       }
     }
   }
@@ -1585,7 +1699,7 @@ int flb_objective_u2(flb_lattice* h, double* J, void* stream) {
       k_objective<S, R><<<grid, 256, 0, st>>>(
           b.L, geom_of(b), static_cast<const S*>(h->pops[h->cur]), h->sp, (R*)nullptr,
           (double*)nullptr, h->red, false);
-      k_sum_partials<<<1, 256, 0, st>>>(h->red, grid, 1, jacc);
+      k_sum_partials_dd<<<1, 256, 0, st>>>(h->red, grid, jacc);
     }
     return FLB_OK;
   });

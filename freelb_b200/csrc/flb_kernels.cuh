@@ -232,6 +232,67 @@ __device__ __forceinline__ double warp_max(double v) {
 // does not depend on CTA scheduling, unlike atomics (~1e-14 relative jitter on
 // a sum of millions of terms, enough to swamp a finite difference of it).
 constexpr int RED_SLOTS = 148 * 32;  // the largest grid_1d grid
+// Error-free addition (Knuth's TwoSum): s + e == a + b exactly, s = fl(a + b).
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+// Compensated (double-double) accumulation: hi + lo carries the running sum
+// with ~2^-106 relative error, so a sum of millions of FP64 terms keeps every
+// digit of the terms (Ogita, Rump & Oishi, SIAM J. Sci. Comput. 26 (2005)).
+struct dd {
+  double hi = 0, lo = 0;
+  __device__ __forceinline__ void add(double v) {
+    double s, e;
+    two_sum(hi, v, s, e);
+    hi = s;
+    lo += e;
+  }
+  __device__ __forceinline__ void add(dd o) {
+    double s, e;
+    two_sum(hi, o.hi, s, e);
+    hi = s;
+    lo += e + o.lo;
+  }
+};
+__device__ __forceinline__ dd warp_sum_dd(dd v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dd w;
+    w.hi = __shfl_xor_sync(0xffffffffu, v.hi, o);
+    w.lo = __shfl_xor_sync(0xffffffffu, v.lo, o);
+    v.add(w);
+  }
+  return v;
+}
+// Slots of (hi, lo) pairs, summed in a fixed order with compensation: acc[0]
+// += the rounded double-double total (k_objective).
+static __global__ void __launch_bounds__(256) k_sum_partials_dd(const double* partials,
+                                                                int nslots, double* acc) {
+  __shared__ double red[2][256];
+  dd s;
+  for (int b = threadIdx.x; b < nslots; b += 256) {
+    dd v;
+    v.hi = partials[2 * b];
+    v.lo = partials[2 * b + 1];
+    s.add(v);
+  }
+  red[0][threadIdx.x] = s.hi;
+  red[1][threadIdx.x] = s.lo;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    dd t;
+    for (int k = 0; k < 256; ++k) {
+      dd v;
+      v.hi = red[0][k];
+      v.lo = red[1][k];
+      t.add(v);
+    }
+    acc[0] += t.hi + t.lo;
+  }
+}
+
 static __global__ void __launch_bounds__(256) k_sum_partials(const double* partials,
                                                              int nslots, int ncomp, double* acc) {
   __shared__ double red[256];

@@ -45,7 +45,7 @@ extern "C" {
 #define FLB_ERR_INVALID (-1)     /* bad argument or descriptor */
 #define FLB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
 #define FLB_ERR_OOM (-3)         /* device allocation failed */
-#define FLB_ERR_TIMEOUT (-4)     /* a bounded device wait gave up */
+#define FLB_ERR_TIMEOUT (-4)     /* a bounded device wait gave up (flb_device_status) */
 #define FLB_ERR_NUMERIC (-5)     /* non-finite population detected */
 #define FLB_ERR_UNSUPPORTED (-6) /* combination not built */
 #define FLB_ERR_STATE (-7)       /* call not valid in the handle's state */
@@ -311,10 +311,33 @@ FLB_API int flb_download_field_block(flb_lattice* lat, int block, int field, voi
  * persistent grid (as many 4-warp CTAs as fit per SM) whose warps copy the next
  * tile's sources into shared memory while the current tile collides; it runs 4
  * cells per thread and ignores tile_y (FLB_ERR_UNSUPPORTED elsewhere).
+ * ctas_per_sm = -2 / -3 selects, for single-block FP16S handles whose rows
+ * start on 16-byte boundaries, the bulk-copy kernel: one CTA per SM in which
+ * one thread stages each tile's 19 source ranges and flags in shared memory
+ * with bulk asynchronous copies (3 / 5 stages) while 15 warps collide the
+ * staged tiles; 4 cells per thread (cells_per_thread 4 or 0; the staged
+ * warps run 2-cell chunks).  Its waits are bounded (flb_set_wait_limit;
+ * flb_device_status reports one that gave up).
  * Defaults: tile_y 4, no persistent grid. */
 FLB_API int flb_set_launch(flb_lattice* lat, int tile_y, int ctas_per_sm, int cells_per_thread);
 FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm,
                            int* cells_per_thread);
+
+/* Device-side failure detection (no reference counterpart: the reference's
+ * CUDA path exit()s on errors, src/utils/cuda_device.h:37-44).  Kernels whose
+ * threads wait on one another (the bulk-copy kernel) bound every wait; a wait
+ * that runs past the limit records FLB_ERR_TIMEOUT in the handle's status word
+ * and the kernel ends early, leaving that step incomplete.
+ * flb_set_wait_limit sets the bound of one wait (seconds, default 2, at most
+ * 60).  flb_device_status synchronises `stream` and returns FLB_OK, or the
+ * recorded code (which it clears). */
+FLB_API int flb_set_wait_limit(flb_lattice* lat, double seconds);
+FLB_API int flb_device_status(flb_lattice* lat, void* stream);
+/* Failure-detection test hook: while `tile` >= 0, the bulk-copy kernel never
+ * signals that tile's stage, so every wait on it runs out after the wait limit
+ * (and the waits behind it after theirs): the path flb_device_status reports,
+ * exercised without a device fault.  -1 (the default) turns it off. */
+FLB_API int flb_test_withhold_tile(flb_lattice* lat, long long tile);
 
 /* Autotuner: times every candidate launch shape for `trial_steps` steps on
  * `stream` (CUDA events) and keeps the fastest.  The trial steps are real
