@@ -115,7 +115,8 @@ struct flb_lattice {
   int halo_mode = FLB_HALO_NORMAL;
   int tile_y = 4;
   int ctas_per_sm = 0;  // -1: the FP16S async-copy pipeline (k_pull_pipe);
-                        // -2 / -3: the FP16S bulk-copy kernel with 3 / 5 stages (k_pull_tma)
+                        // -2 / -3: the FP16S bulk-copy kernel, 2-cell chunks in 5
+                        // stages / 4-cell chunks in 3 stages (k_pull_tma)
   int pipe_ctas = 0;    // resident k_pull_pipe CTAs per SM (0 = not yet queried)
   bool tma_ready = false;  // k_pull_tma shared-memory attributes set
   double wait_s = 2.0;     // bound of one device-side wait (k_pull_tma)
@@ -487,21 +488,23 @@ bool tma_supported(const flb_lattice* h) {
          h->desc.model != FLB_MODEL_BRINKMAN && L.pitch % 8 == 0 && L.pitch - L.nx <= 16;
 }
 
-template <int MODEL, int NS>
+// Launch modes: ctas_per_sm -2 = 2-cell chunks, 5 stages; -3 = 4-cell chunks, 3 stages.
+template <int MODEL, int NS, int CV>
 int tma_attr() {
-  FLB_CUDA(cudaFuncSetAttribute(k_pull_tma<MODEL, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                tma_smem_bytes<NS>()));
+  FLB_CUDA(cudaFuncSetAttribute(k_pull_tma<MODEL, NS, CV>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                tma_smem_bytes<NS, CV>()));
   return FLB_OK;
 }
 
 int tma_prepare(flb_lattice* h) {
   if (h->tma_ready) return FLB_OK;
-  FLB_TRY((tma_attr<MODEL_BGK, 3>()));
-  FLB_TRY((tma_attr<MODEL_BGK, 5>()));
-  FLB_TRY((tma_attr<MODEL_MRT, 3>()));
-  FLB_TRY((tma_attr<MODEL_MRT, 5>()));
-  FLB_TRY((tma_attr<MODEL_LES, 3>()));
-  FLB_TRY((tma_attr<MODEL_LES, 5>()));
+  FLB_TRY((tma_attr<MODEL_BGK, 5, 2>()));
+  FLB_TRY((tma_attr<MODEL_BGK, 3, 4>()));
+  FLB_TRY((tma_attr<MODEL_MRT, 5, 2>()));
+  FLB_TRY((tma_attr<MODEL_MRT, 3, 4>()));
+  FLB_TRY((tma_attr<MODEL_LES, 5, 2>()));
+  FLB_TRY((tma_attr<MODEL_LES, 3, 4>()));
   h->tma_ready = true;
   return FLB_OK;
 }
@@ -554,18 +557,22 @@ void launch_one_step_v(flb_lattice* h, cudaStream_t st) {
   if constexpr (std::is_same<S, __half>::value && V == 4 && MODEL != MODEL_BRINKMAN) {
     if (h->ctas_per_sm <= -2) {  // flb_set_launch admits it only where tma_supported
       const HostBlock& b = h->blocks[0];
+      const int cv = h->ctas_per_sm == -2 ? 2 : 4;
+      const long long cells = (long long)cv * TMA_CHUNKS;
       TmaParams tp{};
-      tp.ntiles = (b.padded() + TMA_CELLS - 1) / TMA_CELLS;
+      tp.ntiles = (b.padded() + cells - 1) / cells;
       tp.status = status_word(h);
       tp.wait_ns = (unsigned long long)(h->wait_s * 1e9);
       tp.drain_ns = std::max(tp.wait_ns, 1000000000ULL);
       tp.withhold = h->withhold;
+      tma_staged_range(cells, b.L.pitch, b.L.ny, b.L.nz, tp.staged_lo, tp.staged_hi);
       const unsigned g = unsigned(std::max(1LL, std::min(tp.ntiles, (long long)h->sm_count)));
-      const StepParams sp = half_step_params<TMA_V>(h);  // 2-cell chunks
-      if (h->ctas_per_sm == -2)
-        k_pull_tma<MODEL, 3><<<g, TMA_THREADS, tma_smem_bytes<3>(), st>>>(sp, tp);
+      if (cv == 2)
+        k_pull_tma<MODEL, 5, 2><<<g, TMA_THREADS, tma_smem_bytes<5, 2>(), st>>>(
+            half_step_params<2>(h), tp);
       else
-        k_pull_tma<MODEL, 5><<<g, TMA_THREADS, tma_smem_bytes<5>(), st>>>(sp, tp);
+        k_pull_tma<MODEL, 3, 4><<<g, TMA_THREADS, tma_smem_bytes<3, 4>(), st>>>(
+            half_step_params<4>(h), tp);
       return;
     }
   }

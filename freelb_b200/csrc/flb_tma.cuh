@@ -14,11 +14,10 @@
 // t*TMA_CELLS + off_i + TMA_CELLS + TMA_HALO) (off_i = -c_y pitch - c_z plane,
 // the source row of direction i) and the tile's flags into one stage of a ring
 // of NS stages, each copy one cp.async.bulk completing on the stage's "full"
-// mbarrier.  Warps 1..15 are consumers: thread (w, l) owns the 2-cell chunk
-// c = 32 (w - 1) + l of the tile (one float2 pair: the loads now live in shared
-// memory, so the pair collision fits the 128 registers a CTA of 16 warps gives
-// it; a second chunk per thread and tile made the compiler keep values live
-// across both and spill), reads the chunk's 19 words from the stage exactly as
+// mbarrier.  Warps 1..15 are consumers: thread (w, l) owns chunk
+// c = 32 (w - 1) + l of the tile, CV = 2 or 4 cells (one chunk per thread and
+// tile: a second one made the compiler keep values live across both and
+// spill), reads the chunk's 19 words from the stage exactly as
 // the direct kernel reads them from global memory (own word, the adjacent word
 // for the x-shifted directions, the row-end fixups, all inside the TMA_HALO
 // margins), collides with collide_half and stores to global memory; then the
@@ -50,20 +49,24 @@ namespace flb {
 
 constexpr int TMA_THREADS = 512;
 constexpr int TMA_CONSUMER_WARPS = TMA_THREADS / 32 - 1;  // 15
-constexpr int TMA_V = 2;                                  // cells per chunk
 constexpr int TMA_CHUNKS = 32 * TMA_CONSUMER_WARPS;      // 480 chunks per tile
-constexpr int TMA_CELLS = TMA_V * TMA_CHUNKS;            // 960 cells per tile
 constexpr int TMA_HALO = 24;                             // halves before / after a range
-constexpr int TMA_DIRH = TMA_CELLS + 2 * TMA_HALO;       // 1008 halves per direction
-constexpr int TMA_DIRB = 2 * TMA_DIRH;                   // 2016 bytes
-constexpr int TMA_STAGE = Q * TMA_DIRB + TMA_CELLS;      // + the tile's flags: 39,264 bytes
-static_assert(TMA_DIRB % 16 == 0 && TMA_STAGE % 16 == 0 && (2 * TMA_HALO) % 16 == 0,
-              "bulk copies need 16-byte sizes and destinations");
-static_assert((2 * TMA_CELLS) % 16 == 0, "tile starts stay 16-byte aligned");
 
-template <int NS>
+// Tile geometry for chunks of CV cells (2 or 4): TMA_CHUNKS chunks per tile.
+template <int CV>
+struct TmaTile {
+  static constexpr int cells = CV * TMA_CHUNKS;        // 960 / 1920 cells per tile
+  static constexpr int dirh = cells + 2 * TMA_HALO;    // halves per direction range
+  static constexpr int dirb = 2 * dirh;                // bytes per direction range
+  static constexpr int stage = Q * dirb + cells;       // + the tile's flags
+  static_assert(dirb % 16 == 0 && stage % 16 == 0 && (2 * TMA_HALO) % 16 == 0,
+                "bulk copies need 16-byte sizes and destinations");
+  static_assert((2 * cells) % 16 == 0, "tile starts stay 16-byte aligned");
+};
+
+template <int NS, int CV>
 constexpr int tma_smem_bytes() {
-  return NS * TMA_STAGE + 2 * NS * 8;  // stages, then the full / empty mbarriers
+  return NS * TmaTile<CV>::stage + 2 * NS * 8;  // stages, then the full / empty mbarriers
 }
 
 // Written to the status word by a wait that gave up (FLB_ERR_TIMEOUT).
@@ -75,6 +78,7 @@ struct TmaParams {
   unsigned long long wait_ns;  // bound of one mbarrier wait of the pipeline
   unsigned long long drain_ns; // bound of the producer's wait for its last copies
   long long withhold;          // failure-detection test: this tile is never signalled (-1: none)
+  long long staged_lo, staged_hi;  // the staged tiles: t in [staged_lo, staged_hi]
 };
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
@@ -127,23 +131,31 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned b
       : "memory");
 }
 
-// Tiles whose ranges stay inside the block and away from the wrap rows: the
-// rows of the tile lie in [ny + 3, ny nz - ny - 4].
-__device__ __forceinline__ bool tma_tile_staged(const StepParams& p, long long t) {
-  const long long c0 = t * TMA_CELLS, c1 = c0 + TMA_CELLS - 1;
-  const long long r0 = c0 / p.pitch, r1 = c1 / p.pitch;
-  return r0 >= p.ny + 3 && r1 <= (long long)p.ny * p.nz - p.ny - 4;
+// Tiles whose ranges stay inside the block and away from the wrap rows are
+// those whose rows lie in [ny + 3, ny nz - ny - 4]: one contiguous range of
+// tiles, computed on the host (tma_staged_range) so that no thread divides.
+__host__ __device__ __forceinline__ void tma_staged_range(long long cells, long long pitch,
+                                                          long long ny, long long nz,
+                                                          long long& lo, long long& hi) {
+  lo = ((ny + 3) * pitch + cells - 1) / cells;
+  const long long num = (ny * nz - ny - 3) * pitch - cells;
+  hi = num >= 0 ? num / cells : -1;
+}
+__device__ __forceinline__ bool tma_tile_staged(const TmaParams& tp, long long t) {
+  return t >= tp.staged_lo && t <= tp.staged_hi;
 }
 
-// The words of 2-cell chunk c (first cell at x0 of its row) of a staged tile
+// The words of CV-cell chunk c (first cell at x0 of its row) of a staged tile
 // in stage `sb`: the same words gather_words_dir reads from global memory.
+template <int CV>
 __device__ __forceinline__ void gather_words_stage(const StepParams& p, const __half* sb, int c,
-                                                   int x0, unsigned (&h)[Q]) {
+                                                   int x0, typename HWord<CV>::type (&h)[Q]) {
+  using W = typename HWord<CV>::type;
+  constexpr int DIRH = TmaTile<CV>::dirh;
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
-    const unsigned* own =
-        reinterpret_cast<const unsigned*>(sb + i * TMA_DIRH + TMA_HALO + TMA_V * c);
-    const unsigned v = own[0];
+    const W* own = reinterpret_cast<const W*>(sb + i * DIRH + TMA_HALO + CV * c);
+    const W v = own[0];
     if (cx(i) == 0) h[i] = v;
     else if (cx(i) > 0) h[i] = hsplice_prev(own[-1], v);
     else h[i] = hsplice_next(v, own[1]);
@@ -152,17 +164,16 @@ __device__ __forceinline__ void gather_words_stage(const StepParams& p, const __
   if (x0 == 0) {  // x = nx-1 of the row before the source row
 #pragma unroll
     for (int i = 1; i < Q; ++i)
-      if (cx(i) > 0)
-        hset(h[i], 0, s16[i * TMA_DIRH + TMA_HALO + TMA_V * c - p.pitch + p.nx - 1]);
+      if (cx(i) > 0) hset(h[i], 0, s16[i * DIRH + TMA_HALO + CV * c - p.pitch + p.nx - 1]);
   }
   const int klast = p.nx - 1 - x0;
-  if (klast >= 0 && klast < TMA_V) {  // x = 0 of the row after the source row
+  if (klast >= 0 && klast < CV) {  // x = 0 of the row after the source row
 #pragma unroll
     for (int i = 1; i < Q; ++i)
       if (cx(i) < 0) {
-        const unsigned e = s16[i * TMA_DIRH + TMA_HALO + TMA_V * c + p.pitch - x0];
+        const unsigned e = s16[i * DIRH + TMA_HALO + CV * c + p.pitch - x0];
 #pragma unroll
-        for (int k = 0; k < TMA_V; ++k)
+        for (int k = 0; k < CV; ++k)
           if (k == klast) hset(h[i], k, e);
       }
   }
@@ -170,16 +181,18 @@ __device__ __forceinline__ void gather_words_stage(const StepParams& p, const __
 
 // Chunks of unstaged tiles: the direct kernel's path, out of line so that its
 // registers do not weigh on the staged path.
-template <int MODEL>
+template <int MODEL, int CV>
 __device__ __noinline__ void tma_direct_chunk(const StepParams& p, float omega, int x0,
                                               unsigned row, unsigned cell) {
-  pull_chunk_half32<MODEL, TMA_V>(p, Geom{p.nx, p.ny, p.nz, p.pitch, p.plane, 0}, omega, x0,
-                                  row, cell);
+  pull_chunk_half32<MODEL, CV>(p, Geom{p.nx, p.ny, p.nz, p.pitch, p.plane, 0}, omega, x0, row,
+                               cell);
 }
 
-template <int MODEL, int NS>
+template <int MODEL, int NS, int CV>
 __global__ void __launch_bounds__(TMA_THREADS, 1)
     k_pull_tma(const __grid_constant__ StepParams p, const TmaParams tp) {
+  constexpr int TMA_CELLS = TmaTile<CV>::cells, TMA_DIRB = TmaTile<CV>::dirb,
+                TMA_STAGE = TmaTile<CV>::stage;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + NS * TMA_STAGE);
   uint64_t* empty = full + NS;
@@ -211,7 +224,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
       unsigned char* st = smem + s * TMA_STAGE;
       if (t == tp.withhold) {
         // nothing arrives on this stage: its consumers' waits run out
-      } else if (tma_tile_staged(p, t)) {
+      } else if (tma_tile_staged(tp, t)) {
         mbar_arrive_tx(&full[s], unsigned(TMA_STAGE));
         const long long c0 = t * TMA_CELLS;
 #pragma unroll 1
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
 
   // consumers
   const float omega = float(p.omega);
-  const unsigned cpr = unsigned(p.pitch) / TMA_V;
+  const unsigned cpr = unsigned(p.pitch) / CV;
   long long k = 0;
   for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
     const int s = int(k % NS);
@@ -245,23 +258,23 @@ __global__ void __launch_bounds__(TMA_THREADS, 1)
       return;
     }
     const int c = (warp - 1) * 32 + lane;
-    const unsigned cell = unsigned(t) * unsigned(TMA_CELLS) + unsigned(TMA_V * c);
-    const unsigned q = cell / TMA_V;
+    const unsigned cell = unsigned(t) * unsigned(TMA_CELLS) + unsigned(CV * c);
+    const unsigned q = cell / CV;
     const unsigned row = p.cpr_m ? __umulhi(q, p.cpr_m) >> (p.cpr_s - 1) : q;
-    const int x0 = int(q - row * cpr) * TMA_V;
+    const int x0 = int(q - row * cpr) * CV;
     if (cell < cells_total && x0 < p.nx) {
-      if (tma_tile_staged(p, t)) {
+      if (tma_tile_staged(tp, t)) {
         const unsigned char* st = smem + s * TMA_STAGE;
-        unsigned h[Q];
-        gather_words_stage(p, reinterpret_cast<const __half*>(st), c, x0, h);
-        const uchar2 fv = reinterpret_cast<const uchar2*>(st + Q * TMA_DIRB)[c];
-        const uint8_t fl[TMA_V] = {fv.x, fv.y};
-        collide_half<MODEL, TMA_V>(p, omega, (long long)cell, fl, h);
+        typename HWord<CV>::type h[Q];
+        gather_words_stage<CV>(p, reinterpret_cast<const __half*>(st), c, x0, h);
+        uint8_t fl[CV];
+        load_flags<CV>(st + Q * TMA_DIRB + CV * c, fl);
+        collide_half<MODEL, CV>(p, omega, (long long)cell, fl, h);
 #pragma unroll
         for (int i = 0; i < Q; ++i)
-          hstore<TMA_V>(static_cast<__half*>(p.dst_dir[i]) + cell, h[i]);
+          hstore<CV>(static_cast<__half*>(p.dst_dir[i]) + cell, h[i]);
       } else {
-        tma_direct_chunk<MODEL>(p, omega, x0, row, cell);
+        tma_direct_chunk<MODEL, CV>(p, omega, x0, row, cell);
       }
     }
     __syncwarp();
