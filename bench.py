@@ -515,7 +515,8 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
 
     # headline: 512^3 BGK FP32, launch shape from the autotuner
-    lat = F.cavity(ni, tau=0.53, ulid=0.1, storage=args.storage)
+    htau = 3 * 0.1 * ni / 10000 + 0.5 if args.model == "les" else 0.53
+    lat = F.cavity(ni, tau=htau, ulid=0.1, storage=args.storage, model=args.model)
     if args.launch:
         launch = tuple(int(v) for v in args.launch.split(","))
         lat.set_launch(*launch)
@@ -642,7 +643,8 @@ def run_ours(args, rank, world, local_rank):
         "dtype": {"fp32": "f32", "fp16s": "f32 (fp16 storage)", "fp64": "f64",
                   "fp32s": "f32 (fp32 deviation storage)"}[args.storage],
         "data": "synthetic",
-        "config": {"workload": f"lid-driven cavity {ni}^3 D3Q19 BGK tau=0.53 u_lid=0.1",
+        "config": {"workload": f"lid-driven cavity {ni}^3 D3Q19 {args.model.upper()} "
+                               f"tau={htau:g} u_lid=0.1",
                    "stored_cells": cells, "storage": args.storage, "per_gpu": "independent cavity",
                    "l2": "working set 21.8 GB >> 126 MB L2; no flush needed",
                    "parallelism": f"replicas x{world}", "launch": launch},
@@ -679,6 +681,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16s", "fp64", "fp32s"],
                     help="population storage of the headline run (profiling)")
+    ap.add_argument("--model", default="bgk", choices=["bgk", "mrt", "les"],
+                    help="collision model of the headline run (profiling; the headline is BGK)")
     ap.add_argument("--launch", default=None,
                     help="tile_y,ctas_per_sm,cells_per_thread for the headline run instead of "
                          "the autotuner (profiling)")

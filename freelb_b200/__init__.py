@@ -229,8 +229,12 @@ class Lattice:
         return v.value
 
     def nonfinite(self, stream=None):
+        """Number of non-finite populations (the C call returns FLB_ERR_NUMERIC
+        when it is not zero)."""
         v = ctypes.c_uint64()
-        C.call("flb_check_finite", self._h, ctypes.byref(v), _stream(stream))
+        rc = C.load().flb_check_finite(self._h, ctypes.byref(v), _stream(stream))
+        if rc not in (C.FLB_OK, C.ERR_NUMERIC):
+            raise C.FlbError(rc, "flb_check_finite", C.load().flb_last_error().decode())
         return int(v.value)
 
     def set_halo_mode(self, mode):

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libflb_b200.so")
 
 FLB_OK = 0
+ERR_NUMERIC, ERR_TIMEOUT = -5, -4
 ERRORS = {-1: "FLB_ERR_INVALID", -2: "FLB_ERR_CUDA", -3: "FLB_ERR_OOM", -4: "FLB_ERR_TIMEOUT",
           -5: "FLB_ERR_NUMERIC", -6: "FLB_ERR_UNSUPPORTED", -7: "FLB_ERR_STATE"}
 

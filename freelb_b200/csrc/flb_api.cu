@@ -1664,6 +1664,7 @@ int flb_check_finite(flb_lattice* h, uint64_t* bad, void* stream) {
   FLB_CUDA(cudaMemcpyAsync(&v, acc, sizeof v, cudaMemcpyDeviceToHost, st));
   FLB_CUDA(cudaStreamSynchronize(st));
   *bad = v;
+  if (v) return fail(FLB_ERR_NUMERIC, "%llu non-finite populations", v);
   return FLB_OK;
 }
 

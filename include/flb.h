@@ -46,7 +46,7 @@ extern "C" {
 #define FLB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
 #define FLB_ERR_OOM (-3)         /* device allocation failed */
 #define FLB_ERR_TIMEOUT (-4)     /* a bounded device wait gave up (flb_device_status) */
-#define FLB_ERR_NUMERIC (-5)     /* non-finite population detected */
+#define FLB_ERR_NUMERIC (-5)     /* non-finite population detected (flb_check_finite) */
 #define FLB_ERR_UNSUPPORTED (-6) /* combination not built */
 #define FLB_ERR_STATE (-7)       /* call not valid in the handle's state */
 
@@ -237,7 +237,8 @@ FLB_API int flb_reduce_conservation(flb_lattice* lat, uint8_t key, double out[4]
  * BlockLattice::getToleranceU (block_lattice.hh:266-288). */
 FLB_API int flb_tolerance_u(flb_lattice* lat, uint8_t key, double* max_du, void* stream);
 
-/* Non-finite check of the populations: *bad = number of non-finite values. */
+/* Non-finite check of the populations: *bad = number of non-finite values;
+ * returns FLB_ERR_NUMERIC when that number is not zero. */
 FLB_API int flb_check_finite(flb_lattice* lat, uint64_t* bad, void* stream);
 
 /* Device pointers for zero-copy consumers: populations (current buffer),

@@ -164,3 +164,21 @@ def test_conservation_and_tolerance(gpu_ok):
     lat.step(1)
     assert lat.tolerance_u(key=2) > 0.0
     assert lat.nonfinite() == 0
+
+
+def test_non_finite_populations_are_reported(gpu_ok):
+    """flb_check_finite counts non-finite populations and returns
+    FLB_ERR_NUMERIC when there are any (a NaN uploaded on the host; stepping it
+    only spreads the NaN)."""
+    import ctypes
+    from freelb_b200 import _capi as C
+    lat = F.cavity(10)
+    pops = lat.download_pops()
+    assert lat.nonfinite() == 0
+    pops[5 * lat.N + 123] = np.nan
+    lat.upload_pops(pops)
+    v = ctypes.c_uint64()
+    rc = C.load().flb_check_finite(lat._h, ctypes.byref(v), None)
+    assert rc == C.ERR_NUMERIC and v.value == 1
+    lat.step(2)
+    assert lat.nonfinite() > 1
