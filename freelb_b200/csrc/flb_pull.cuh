@@ -534,6 +534,112 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
   }
 }
 
+// MRT on deviations for two cells at once (the pair form of bgk_deviation2):
+// the non-equilibrium part N = H - E in stored units, the 15 non-conserved
+// moments of N, their relaxation and the back-transform, every operation one
+// two-wide FP32 instruction (explicit fma2 / add2 / mul2, no contraction left
+// to the compiler), so each cell's result is the same whichever cell shares
+// its pair.  Every FP16S MRT bulk cell goes through it (a lone one on a
+// duplicated lane).
+__device__ __forceinline__ void mrt_deviation2(const StepParams& p, float2 (&H)[Q], float omega) {
+  float2 sp[Q], df[Q];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = add2(H[i], H[i + 1]);
+    df[i] = sub2(H[i], H[i + 1]);
+  }
+  const float2 sum = add2(add2(add2(add2(H[0], sp[1]), add2(sp[3], sp[5])),
+                               add2(add2(sp[7], sp[9]), add2(sp[11], sp[13]))),
+                          add2(sp[15], sp[17]));
+  const float2 mx = add2(add2(add2(df[1], df[7]), add2(df[9], df[13])), df[15]);
+  const float2 my = add2(add2(add2(df[3], df[7]), sub2(df[11], df[13])), df[17]);
+  const float2 mz = sub2(add2(add2(df[5], df[9]), sub2(df[11], df[15])), df[17]);
+  const float2 delta = mul2(sum, p2(p.inv_scale));
+  const float2 rho = add2(p2(p.rho0), delta);
+  const float2 ir = make_float2(__fdividef(p.inv_scale, rho.x), __fdividef(p.inv_scale, rho.y));
+  const float2 ux = mul2(mx, ir), uy = mul2(my, ir), uz = mul2(mz, ir);
+  const float2 q = mul2(p2(-1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
+  const float2 k1 = mul2(p2(3.0f), ux), k3 = mul2(p2(3.0f), uy), k5 = mul2(p2(3.0f), uz);
+  float2 k[Q];
+  k[1] = k1;
+  k[3] = k3;
+  k[5] = k5;
+  k[7] = add2(k1, k3);
+  k[9] = add2(k1, k5);
+  k[11] = add2(k3, k5);
+  k[13] = sub2(k1, k3);
+  k[15] = sub2(k1, k5);
+  k[17] = sub2(k3, k5);
+  // N_i = H_i - S w_i (delta + rho g_i); pair sums a and differences b of N
+  const float s0 = p.scale * (1.0f / 3.0f), s1 = p.scale * (1.0f / 18.0f),
+              s2 = p.scale * (1.0f / 36.0f);
+  const float2 n0 = fma2(p2(-s0), fma2(rho, q, delta), H[0]);
+  float2 a[9], b[9];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float sw = i < 7 ? s1 : s2;
+    const float2 e = fma2(mul2(p2(0.5f), k[i]), k[i], q);
+    const float2 n1 = fma2(p2(-sw), fma2(rho, add2(e, k[i]), delta), H[i]);
+    const float2 n2 = fma2(p2(-sw), fma2(rho, sub2(e, k[i]), delta), H[i + 1]);
+    a[i / 2] = add2(n1, n2);
+    b[i / 2] = sub2(n1, n2);
+  }
+  // mu_k = s_k / |M_k|^2 * (M_k . N) over the non-conserved moments
+  float2 mu[Q];
+#pragma unroll
+  for (int kk = 0; kk < Q; ++kk) {
+    if (mrt_conserved(kk)) {
+      mu[kk] = p2(0.0f);
+      continue;
+    }
+    float2 m = p2(0.0f);
+    if (mrt_even(kk)) {
+      if (mrt_m(kk, 0) != 0) m = mul2(p2(float(mrt_m(kk, 0))), n0);
+#pragma unroll
+      for (int pp = 0; pp < 9; ++pp) {
+        const int c = mrt_m(kk, 2 * pp + 1);
+        if (c == 1) m = add2(m, a[pp]);
+        else if (c == -1) m = sub2(m, a[pp]);
+        else if (c != 0) m = fma2(p2(float(c)), a[pp], m);
+      }
+    } else {
+#pragma unroll
+      for (int pp = 0; pp < 9; ++pp) {
+        const int c = mrt_m(kk, 2 * pp + 1);
+        if (c == 1) m = add2(m, b[pp]);
+        else if (c == -1) m = sub2(m, b[pp]);
+        else if (c != 0) m = fma2(p2(float(c)), b[pp], m);
+      }
+    }
+    const float sk = mrt_shear(kk) ? omega * (1.0f / float(mrt_norm_lit(kk)))
+                                   : float(p.s_over_norm[kk]);
+    mu[kk] = mul2(m, p2(sk));
+  }
+  // back-transform: H_i -= sum_k M[k][i] mu_k
+  float2 d0 = p2(0.0f);
+#pragma unroll
+  for (int kk = 0; kk < Q; ++kk)
+    if (mrt_even(kk) && !mrt_conserved(kk) && mrt_m(kk, 0) != 0)
+      d0 = fma2(p2(float(mrt_m(kk, 0))), mu[kk], d0);
+  H[0] = sub2(H[0], d0);
+#pragma unroll
+  for (int pp = 0; pp < 9; ++pp) {
+    float2 e = p2(0.0f), o = p2(0.0f);
+#pragma unroll
+    for (int kk = 0; kk < Q; ++kk) {
+      if (mrt_conserved(kk)) continue;
+      const int c = mrt_m(kk, 2 * pp + 1);
+      if (c == 0) continue;
+      if (mrt_even(kk)) e = c == 1 ? add2(e, mu[kk]) : c == -1 ? sub2(e, mu[kk])
+                                                               : fma2(p2(float(c)), mu[kk], e);
+      else o = c == 1 ? add2(o, mu[kk]) : c == -1 ? sub2(o, mu[kk])
+                                                  : fma2(p2(float(c)), mu[kk], o);
+    }
+    H[2 * pp + 1] = sub2(H[2 * pp + 1], add2(e, o));
+    H[2 * pp + 2] = sub2(H[2 * pp + 2], sub2(e, o));
+  }
+}
+
 // MRT (collision::MRT_Feq_RhoU) on deviations: H <- H - M^-1 S M N, given the
 // non-equilibrium part N.
 __device__ __forceinline__ void mrt_relax_neq(const StepParams& p, float (&H)[Q], float omega,
@@ -549,12 +655,6 @@ __device__ __forceinline__ void mrt_relax_neq(const StepParams& p, float (&H)[Q]
   for (int k = 0; k < Q; ++k)
     s[k] = mrt_shear(k) ? omega * (1.0f / float(mrt_norm_lit(k))) : float(p.s_over_norm[k]);
   mrt_relax<float>(H, N[0], a, b, s);
-}
-
-__device__ __forceinline__ void mrt_deviation(const StepParams& p, float (&H)[Q], float omega) {
-  float rho, N[Q];
-  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
-  mrt_relax_neq(p, H, omega, N);
 }
 
 // Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
@@ -727,7 +827,12 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
   if (op == OP_NONE) return;
   if constexpr (MODEL == MODEL_MRT) {
     if (op == OP_BULK) {
-      mrt_deviation(p, H, omega);
+      float2 H2[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H2[i] = p2(H[i]);
+      mrt_deviation2(p, H2, omega);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H[i] = H2[i].x;
       return;
     }
   }
@@ -766,14 +871,15 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
   for (int k = 0; k < V; k += 2) {
     const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
     if (opa == OP_NONE && opb == OP_NONE) continue;
-    if (MODEL == MODEL_BGK && opa == OP_BULK && opb == OP_BULK) {
+    if ((MODEL == MODEL_BGK || MODEL == MODEL_MRT) && opa == OP_BULK && opb == OP_BULK) {
       float2 H2[Q];
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
         const unsigned q = hpart(h[i], k);
         H2[i] = __half22float2(*reinterpret_cast<const __half2*>(&q));
       }
-      bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
+      if constexpr (MODEL == MODEL_MRT) mrt_deviation2(p, H2, omega);
+      else bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
         const __half2 r = __float22half2_rn(H2[i]);
@@ -975,14 +1081,14 @@ __device__ __forceinline__ bool chunk_coords(const Geom& g, long long q, int& x0
 // only padding lanes idle.  Grid: ceil(chunks / blockDim.x) CTAs.
 // Minimum resident 256-thread CTAs per SM asked of the compiler, i.e. the
 // register cap: 3 (85 registers, 24 warps per SM) for the FP32 kernels at 2
-// cells per thread and the FP16S MRT / LES kernels, 2 (128 registers) for FP16S
-// BGK (its two-wide pair code spills badly at 85) and FP32 at 4 cells per
-// thread; FP64 is left free.  Measured at 512^3 against the other caps.
+// cells per thread and the FP16S LES kernel, 2 (128 registers) for FP16S BGK
+// and MRT (their two-wide pair code spills badly at 85) and FP32 at 4 cells
+// per thread; FP64 is left free.  Measured at 512^3 against the other caps.
 template <typename S, int MODEL, int V>
 struct PullBounds {
   static constexpr int min_ctas =
       std::is_same<S, double>::value                          ? 1
-      : std::is_same<S, __half>::value && MODEL == MODEL_BGK ? 2
+      : std::is_same<S, __half>::value && (MODEL == MODEL_BGK || MODEL == MODEL_MRT) ? 2
       : (std::is_same<S, float>::value || std::is_same<S, dev32>::value) && V == 4 ? 2
                                                               : 3;
 };
