@@ -228,15 +228,33 @@ def timed_cavity(F, torch, stream, ni, steps, warmup, storage="fp32", model="bgk
     return t.ms, launch, lat
 
 
-def accuracy_block(F, ni, steps, keep_bgk_fp32=False):
+W19 = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+
+def round_once_fp16s(pops):
+    """Every population's deviation from its lattice weight rounded once, in
+    place, to FP16S precision: binary16 of (f - w) * 2^10, read back in FP64
+    (direction by direction, in 16M-cell pieces, so a 512^3 lattice needs no
+    second full-size host array)."""
+    p = pops.reshape(19, -1)
+    for i, wi in enumerate(W19):
+        for s in range(0, p.shape[1], 1 << 24):
+            seg = p[i, s:s + (1 << 24)]
+            seg[:] = ((seg - wi) * 1024.0).astype(np.float16).astype(np.float64) / 1024.0 + wi
+
+
+def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les")):
     """Relative L2 error of u after `steps` steps against an FP64 run of the same
-    kernel, per model and storage (C2 accuracy report).  LES also reports the
-    spread of two FP64 runs whose initial populations differ by 1e-7 (relative,
-    seeded): the flow's own sensitivity, beside which the storage errors read.
-    With keep_bgk_fp32 the FP32 BGK populations (reference order) are returned
-    for the parity check against the reference's own FP32 run."""
+    kernel, per model and storage (C2 accuracy report).  Beside it, the flow's
+    own sensitivity: an FP64 run whose populations are rounded once to FP16S
+    precision at step steps/2 (FP16S storage rounds at that precision every
+    step), and for LES two FP64 runs whose initial populations differ by 1e-7
+    and 2^-12 (relative, seeded).  With keep_bgk_fp32 the FP32 BGK populations
+    (reference order) are returned for the parity check against the
+    reference's own FP32 run."""
     out, kept = {}, None
-    for model, tau in (("bgk", 0.53), ("mrt", 0.53), ("les", 3 * 0.1 * ni / 10000 + 0.5)):
+    taus = {"bgk": 0.53, "mrt": 0.53, "les": 3 * 0.1 * ni / 10000 + 0.5}
+    for model, tau in ((m, taus[m]) for m in models):
         us = {}
         for storage in ("fp64", "fp32", "fp32s", "fp16s"):
             lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model)
@@ -251,11 +269,22 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False):
                                      for s in ("fp32", "fp32s", "fp16s")}}
         if keep_bgk_fp32 and model == "bgk":
             kept = kept + (us["fp64"],)
+        lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
+        lat.step(steps // 2)
+        pops = lat.download_pops(np.float64)
+        round_once_fp16s(pops)
+        lat.upload_pops(pops)
+        del pops
+        lat.step(steps - steps // 2)
+        _, u = lat.rhou(key=2, dtype=np.float64)
+        lat.close()
+        out[model]["fp64_one_fp16s_rounding_rel_l2_u"] = float(np.linalg.norm(u - us["fp64"]) / ref)
+        del u
         if model == "les":
             # FP64 runs from initial populations perturbed by eps (relative,
             # seeded): 1e-7, and 2^-12, the rounding of one FP16 store
             n = ni + 2
-            w = np.repeat(np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12), n ** 3)
+            w = np.repeat(W19, n ** 3)
             xi = np.random.default_rng(123).standard_normal(19 * n ** 3)
             for name, eps in (("1e-7", 1e-7), ("2^-12", 2.0 ** -12)):
                 lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
@@ -600,7 +629,8 @@ def run_ours(args, rank, world, local_rank):
                 "glups": cells * args.steps / (ms / 1e3) / 1e9, "frac": ach / measured_peaks()[0],
                 "launch": lch, "nonfinite": bad}
         extras["variants"] = variants
-        acc = accuracy_block(F, args.accuracy_ni, 2000, keep_bgk_fp32=args.accuracy_ni == par_ni)
+        acc = accuracy_block(F, args.accuracy_ni, 2000, keep_bgk_fp32=args.accuracy_ni == par_ni,
+                             models=tuple(args.accuracy_models.split(",")))
         extras["accuracy"], kept = acc if isinstance(acc, tuple) else (acc, None)
         extras["blocks_256"] = blocks_block(F, torch, stream, 256, args.steps)
         extras["ensemble_128"] = ensemble_block(F, torch, stream)
@@ -689,14 +719,17 @@ def main():
                          "the autotuner (profiling)")
     ap.add_argument("--accuracy-ni", type=int, default=256,
                     help="cavity size of the FP64-referenced velocity error report (256 or 512)")
+    ap.add_argument("--accuracy-models", default="bgk,mrt,les",
+                    help="models of the velocity error report (comma-separated)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the 256^3 parity runs of the reference's CPU path (background)")
     ap.add_argument("--quick", action="store_true",
                     help="headline and e2e only (no variants / accuracy / blocks / ensemble / "
                          "adjoint blocks)")
-    ap.add_argument("--only", default=None, choices=["blocks", "ensemble"],
+    ap.add_argument("--only", default=None, choices=["blocks", "ensemble", "accuracy"],
                     help="run one secondary workload alone and print its JSON (profiling): "
-                         "the 48 uneven blocks of the 256^3 cavity or the 128-cavity ensemble")
+                         "the 48 uneven blocks of the 256^3 cavity, the 128-cavity ensemble, "
+                         "or the velocity error report at --accuracy-ni")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -711,6 +744,9 @@ def main():
         stream = torch.cuda.current_stream()
         if args.only == "blocks":
             out = {"blocks_256": blocks_block(F, torch, stream, 256, args.steps)}
+        elif args.only == "accuracy":
+            out = {"accuracy": accuracy_block(F, args.accuracy_ni, 2000,
+                                              models=tuple(args.accuracy_models.split(",")))}
         else:
             out = {"ensemble_128": ensemble_block(F, torch, stream)}
         print(json.dumps(out), flush=True)
