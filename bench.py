@@ -214,10 +214,11 @@ class DeviceTimer:
 
 
 def timed_cavity(F, torch, stream, ni, steps, warmup, storage="fp32", model="bgk", tune=True,
-                 tau=0.53, smagorinsky=0.1):
+                 tau=0.53, smagorinsky=0.1, rounding="default"):
     """Cavity of ni^3 interior cells: autotune the launch shape (the tuning steps
     are real warm-up steps), then time `steps` steps.  Returns (ms, launch, lat)."""
     lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model, smagorinsky=smagorinsky)
+    lat.set_rounding(rounding)
     launch = None
     if tune:
         launch, _, _ = lat.autotune(trial_steps=2, stream=stream)
@@ -256,8 +257,10 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les
     taus = {"bgk": 0.53, "mrt": 0.53, "les": 3 * 0.1 * ni / 10000 + 0.5}
     for model, tau in ((m, taus[m]) for m in models):
         us = {}
-        for storage in ("fp64", "fp32", "fp32s", "fp16s"):
-            lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage, model=model)
+        other = {"mrt": "nearest", "bgk": "stochastic"}.get(model)
+        for storage in ("fp64", "fp32", "fp32s", "fp16s") + (("fp16s_" + other,) if other else ()):
+            lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage.split("_")[0], model=model)
+            lat.set_rounding(other if "_" in storage else "default")
             lat.step(steps)
             _, u = lat.rhou(key=2, dtype=np.float64)
             us[storage] = u
@@ -266,7 +269,8 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les
             lat.close()
         ref = np.linalg.norm(us["fp64"])
         out[model] = {"tau": tau, **{f"{s}_rel_l2_u": float(np.linalg.norm(us[s] - us["fp64"]) / ref)
-                                     for s in ("fp32", "fp32s", "fp16s")}}
+                                     for s in us if s != "fp64"}}
+        out[model]["fp16s_rounding"] = "stochastic" if model == "mrt" else "nearest"
         if keep_bgk_fp32 and model == "bgk":
             kept = kept + (us["fp64"],)
         lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
@@ -615,19 +619,28 @@ def run_ours(args, rank, world, local_rank):
         # other models and storages on the same 512^3 cavity
         variants = {}
         les_tau = 3 * 0.1 * ni / 10000 + 0.5
-        for storage, model, tau in (("fp16s", "bgk", 0.53), ("fp32", "mrt", 0.53),
-                                    ("fp16s", "mrt", 0.53), ("fp32", "les", les_tau),
-                                    ("fp16s", "les", les_tau), ("fp64", "bgk", 0.53),
-                                    ("fp32s", "bgk", 0.53)):
+        for storage, model, tau, rnd in (("fp16s", "bgk", 0.53, "default"),
+                                         ("fp16s", "bgk", 0.53, "stochastic"),
+                                         ("fp32", "mrt", 0.53, "default"),
+                                         ("fp16s", "mrt", 0.53, "default"),
+                                         ("fp16s", "mrt", 0.53, "nearest"),
+                                         ("fp32", "les", les_tau, "default"),
+                                         ("fp16s", "les", les_tau, "default"),
+                                         ("fp64", "bgk", 0.53, "default"),
+                                         ("fp32s", "bgk", 0.53, "default")):
             ms, lch, vl = timed_cavity(F, torch, stream, ni, args.steps, 2, storage, model,
-                                       tau=tau)
+                                       tau=tau, rounding=rnd)
             bad = vl.nonfinite()
+            used = vl.rounding()
             vl.close()
             b = algo_bytes_per_cell(storage)
             ach = cells * b / (ms / args.steps / 1e3) / 1e9
-            variants[f"{model}_{storage}"] = {
+            key = f"{model}_{storage}" + ("" if rnd == "default" else f"_{rnd}")
+            variants[key] = {
                 "glups": cells * args.steps / (ms / 1e3) / 1e9, "frac": ach / measured_peaks()[0],
                 "launch": lch, "nonfinite": bad}
+            if storage == "fp16s":
+                variants[key]["rounding"] = used
         extras["variants"] = variants
         acc = accuracy_block(F, args.accuracy_ni, 2000, keep_bgk_fp32=args.accuracy_ni == par_ni,
                              models=tuple(args.accuracy_models.split(",")))

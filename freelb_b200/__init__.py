@@ -190,6 +190,19 @@ class Lattice:
         """Bound of one device-side wait of the bulk-copy kernel (seconds)."""
         C.call("flb_set_wait_limit", self._h, float(seconds))
 
+    def set_rounding(self, mode):
+        """Rounding of FP16S stores: "nearest", "stochastic" or "default"
+        (stochastic for MRT, nearest otherwise)."""
+        m = {"default": C.ROUND_DEFAULT, "nearest": C.ROUND_NEAREST,
+             "stochastic": C.ROUND_STOCHASTIC}[mode]
+        C.call("flb_set_rounding", self._h, m)
+
+    def rounding(self):
+        """The FP16S rounding in effect: "nearest" or "stochastic"."""
+        v = ctypes.c_int()
+        C.call("flb_get_rounding", self._h, ctypes.byref(v))
+        return "stochastic" if v.value == C.ROUND_STOCHASTIC else "nearest"
+
     def device_status(self, stream=None):
         """Raise FlbError(FLB_ERR_TIMEOUT) if a device-side wait gave up since
         the last check (and clear it)."""

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libflb_b200.so")
 
 FLB_OK = 0
 ERR_NUMERIC, ERR_TIMEOUT = -5, -4
+ROUND_DEFAULT, ROUND_NEAREST, ROUND_STOCHASTIC = -1, 0, 1
 ERRORS = {-1: "FLB_ERR_INVALID", -2: "FLB_ERR_CUDA", -3: "FLB_ERR_OOM", -4: "FLB_ERR_TIMEOUT",
           -5: "FLB_ERR_NUMERIC", -6: "FLB_ERR_UNSUPPORTED", -7: "FLB_ERR_STATE"}
 
@@ -94,6 +95,8 @@ SIGNATURES = {
     "flb_set_wait_limit": [_P, ctypes.c_double],
     "flb_device_status": [_P, _P],
     "flb_test_withhold_tile": [_P, ctypes.c_longlong],
+    "flb_set_rounding": [_P, _I],
+    "flb_get_rounding": [_P, ctypes.POINTER(_I)],
     "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)],
     "flb_step_graph": [_P, _I, _P],

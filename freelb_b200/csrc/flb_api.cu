@@ -122,6 +122,7 @@ struct flb_lattice {
   double wait_s = 2.0;     // bound of one device-side wait (k_pull_tma)
   long long withhold = -1; // failure-detection test hook (flb_test_withhold_tile)
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
+  int rounding = FLB_ROUND_DEFAULT;  // FP16S stores (flb_set_rounding)
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   // Brinkman porosity (FLB_FIELD_ALPHA), arithmetic type
@@ -264,6 +265,15 @@ void build_params(flb_lattice* h) {
   p.scale = fp32s ? 1.0f : 1024.0f;
   p.inv_scale = fp32s ? 1.0f : 1.0f / 1024.0f;
   p.rho0 = float(d.rho0);
+  // FP16S rounding: stochastic for MRT unless the caller chose (its round to
+  // nearest drifts, see the cvt.rs helpers of the step kernels)
+  const int r = h->rounding == FLB_ROUND_DEFAULT
+                    ? (d.model == FLB_MODEL_MRT ? FLB_ROUND_STOCHASTIC : FLB_ROUND_NEAREST)
+                    : h->rounding;
+  p.fp16_round = d.storage == FLB_STORAGE_FP16S && r == FLB_ROUND_STOCHASTIC &&
+                         (d.model == FLB_MODEL_BGK || d.model == FLB_MODEL_MRT)
+                     ? 1
+                     : 0;
 }
 
 // Cells per thread of the pull kernel (launch parameter; defaults are the
@@ -1450,6 +1460,28 @@ int flb_set_wait_limit(flb_lattice* h, double seconds) {
     return fail(FLB_ERR_INVALID, "wait limit %g s outside [0, 60]", seconds);
   h->wait_s = seconds;
   drop_graphs(h);  // the captured launches carry the old limit
+  return FLB_OK;
+}
+
+int flb_set_rounding(flb_lattice* h, int mode) {
+  if (!h) return fail(FLB_ERR_INVALID, "null handle");
+  if (mode != FLB_ROUND_DEFAULT && mode != FLB_ROUND_NEAREST && mode != FLB_ROUND_STOCHASTIC)
+    return fail(FLB_ERR_INVALID, "rounding mode %d", mode);
+  if (mode == FLB_ROUND_STOCHASTIC && h->desc.storage == FLB_STORAGE_FP16S &&
+      h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_MRT)
+    return fail(FLB_ERR_UNSUPPORTED, "stochastic FP16S rounding is built for BGK and MRT");
+  h->rounding = mode;
+  const StepParams keep = h->sp;
+  build_params(h);
+  h->sp.src = keep.src;
+  h->sp.dst = keep.dst;
+  drop_graphs(h);  // the captured launches carry the old mode
+  return FLB_OK;
+}
+
+int flb_get_rounding(const flb_lattice* h, int* mode) {
+  if (!h || !mode) return fail(FLB_ERR_INVALID, "null argument");
+  *mode = h->sp.fp16_round ? FLB_ROUND_STOCHASTIC : FLB_ROUND_NEAREST;
   return FLB_OK;
 }
 

@@ -55,6 +55,7 @@ struct StepParams {
   float shift[Q];     // FP16S: rho0 * w_i
   float scale, inv_scale;
   float rho0;         // FP16S: density of the shift
+  int fp16_round;     // FP16S stores: 0 round to nearest, 1 stochastic (cvt.rs)
 };
 
 // First task whose key shares a bit with the flag (src/utils/tmp.h:283-309),

@@ -861,6 +861,51 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
   for (int i = 0; i < Q; ++i) H[i] = fmaf(f[i], p.scale, -p.shift[i] * p.scale);
 }
 
+// Stochastic rounding of FP16S stores.  cvt.rs.f16x2.f32 (sm_100a) adds a
+// random fraction of the last kept bit to each value's magnitude and then
+// truncates, so E[stored] = value: bits [12:0] of its random word are the
+// fraction of the low half, bits [28:16] that of the high half.  Round to
+// nearest can make the same error step after step where the flow changes
+// slowly, and that error adds up: MRT FP16S on the 512^3 cavity drifts
+// linearly to a velocity error of 1.2e-3 against FP64 after 2000 steps (BGK
+// stays at 3.2e-4; its modes of rate 1/tau ~ 1.9 flip sign every step, MRT's
+// other rates of 1.2 barely do), and stochastic rounding removes the drift.
+// The random fraction of a cell comes from a hash of four of the binary16
+// values it pulled (directions 0, 1, 9, 18), XORed with a per-direction key
+// that has the same 13 bits in both fields.  Those inputs are the same bits in
+// every kernel (the FP32 collision results need not be: a one-ulp difference
+// of a fused multiply-add would change a hash of them entirely), a cell's bits
+// do not depend on the cell it is paired with or on its half, so every FP16S
+// kernel still gives the same result.  The inputs change from step to step
+// because the neighbours' stores are themselves rounded at random; only a
+// state that needs no rounding at all (a fluid at rest) stays put.  A value
+// that is already a binary16 number (a cell without an op) is stored unchanged.
+__device__ __forceinline__ unsigned sr_hash(unsigned a, unsigned b) {
+  unsigned h = a * 0x9e3779b9u ^ b;
+  h ^= h >> 15;
+  h *= 0x2c1b3c6du;
+  h ^= h >> 12;
+  return h;
+}
+__device__ __forceinline__ constexpr unsigned sr_key(int i) {
+  return ((0x9e3u * unsigned(i) + 0x3b5u) & 0x1fffu) * 0x00010001u;
+}
+// lo -> low half, hi -> high half (the order of __floats2half2_rn)
+__device__ __forceinline__ unsigned cvt_rs_half2(float lo, float hi, unsigned rbits) {
+  unsigned d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+  return d;
+}
+// Random word of a pair from its pulled words w0, w1, w9, w18 (directions 0,
+// 1, 9, 18; low halves = cell a, high halves = cell b): low field from cell
+// a's hash, high field from cell b's.
+__device__ __forceinline__ unsigned sr_pair(unsigned w0, unsigned w1, unsigned w9,
+                                            unsigned w18) {
+  const unsigned ha = sr_hash(__byte_perm(w0, w1, 0x5410), __byte_perm(w9, w18, 0x5410));
+  const unsigned hb = sr_hash(__byte_perm(w0, w1, 0x7632), __byte_perm(w9, w18, 0x7632));
+  return __byte_perm(ha, hb, 0x5410);
+}
+
 // Collide one FP16S chunk in place, cells processed in pairs (the two halves
 // of a 32-bit part); fl holds the V cells' flags.
 template <int MODEL, int V>
@@ -871,6 +916,12 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
   for (int k = 0; k < V; k += 2) {
     const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
     if (opa == OP_NONE && opb == OP_NONE) continue;
+    // stochastic rounding is built for BGK and MRT (LES, instruction-bound,
+    // keeps round to nearest and no trace of the other mode)
+    constexpr bool kSR = MODEL == MODEL_BGK || MODEL == MODEL_MRT;
+    const bool sr = kSR && p.fp16_round;
+    unsigned c = 0u;
+    if (sr) c = sr_pair(hpart(h[0], k), hpart(h[1], k), hpart(h[9], k), hpart(h[18], k));
     if ((MODEL == MODEL_BGK || MODEL == MODEL_MRT) && opa == OP_BULK && opb == OP_BULK) {
       float2 H2[Q];
 #pragma unroll
@@ -880,10 +931,15 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
       }
       if constexpr (MODEL == MODEL_MRT) mrt_deviation2(p, H2, omega);
       else bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
+      if (sr) {
 #pragma unroll
-      for (int i = 0; i < Q; ++i) {
-        const __half2 r = __float22half2_rn(H2[i]);
-        hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+        for (int i = 0; i < Q; ++i) hpart(h[i], k) = cvt_rs_half2(H2[i].x, H2[i].y, c ^ sr_key(i));
+      } else {
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+          const __half2 r = __float22half2_rn(H2[i]);
+          hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+        }
       }
       continue;
     }
@@ -897,11 +953,17 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
     }
     collide_deviation<MODEL>(p, opa, a, cell0 + k, omega);
     collide_deviation<MODEL>(p, opb, b, cell0 + k + 1, omega);
+    // a cell without an op round-trips exactly (half -> float -> half), in
+    // either rounding
+    if (sr) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-      // a cell without an op round-trips exactly (half -> float -> half)
-      const __half2 r = __floats2half2_rn(a[i], b[i]);
-      hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+      for (int i = 0; i < Q; ++i) hpart(h[i], k) = cvt_rs_half2(a[i], b[i], c ^ sr_key(i));
+    } else {
+#pragma unroll
+      for (int i = 0; i < Q; ++i) {
+        const __half2 r = __floats2half2_rn(a[i], b[i]);
+        hpart(h[i], k) = *reinterpret_cast<const unsigned*>(&r);
+      }
     }
   }
 }

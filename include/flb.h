@@ -334,6 +334,26 @@ FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm
  * recorded code (which it clears). */
 FLB_API int flb_set_wait_limit(flb_lattice* lat, double seconds);
 FLB_API int flb_device_status(flb_lattice* lat, void* stream);
+/* Rounding of FP16S stores (no reference counterpart: the reference stores
+ * populations in T).  FLB_ROUND_NEAREST rounds every stored deviation to the
+ * nearest binary16 value; FLB_ROUND_STOCHASTIC rounds it up or down with the
+ * probabilities that make the stored value exact on average (the sm_100a
+ * cvt.rs conversion; the random bits come from a hash of the cell's own
+ * post-collision values, so runs are reproducible and every kernel gives the
+ * same bits).  Round to nearest makes the same error step after step where
+ * the flow changes slowly, and in MRT that error accumulates (the 512^3 cavity
+ * ends 1.2e-3 from FP64 after 2000 steps, 3.7e-4 with stochastic rounding).
+ * FLB_ROUND_DEFAULT (the default) is stochastic for MRT and round to nearest
+ * otherwise.  Stochastic rounding is built for the BGK and MRT step kernels
+ * (FLB_ERR_UNSUPPORTED for an FP16S LES or Brinkman handle, which always
+ * round to nearest); other storages ignore the mode.  flb_get_rounding
+ * returns the mode in effect (NEAREST or STOCHASTIC). */
+#define FLB_ROUND_DEFAULT (-1)
+#define FLB_ROUND_NEAREST 0
+#define FLB_ROUND_STOCHASTIC 1
+FLB_API int flb_set_rounding(flb_lattice* lat, int mode);
+FLB_API int flb_get_rounding(const flb_lattice* lat, int* mode);
+
 /* Failure-detection test hook: while `tile` >= 0, the bulk-copy kernel never
  * signals that tile's stage, so every wait on it runs out after the wait limit
  * (and the waits behind it after theirs): the path flb_device_status reports,
