@@ -54,8 +54,10 @@ def make_desc(nx, ny, nz, tau, storage="fp32", model="bgk", smagorinsky=0.1, mrt
     if omega is not None:
         d.omega = float(omega)
     d.smagorinsky = float(smagorinsky)
+    rates = [float(mrt_rate)] * 19 if np.isscalar(mrt_rate) else [float(r) for r in mrt_rate]
+    assert len(rates) == 19, "mrt_rate: one rate or 19 (moment order of the D3Q19 basis)"
     for k in range(19):
-        d.mrt_rates[k] = float(mrt_rate)
+        d.mrt_rates[k] = rates[k]
     d.rho0 = float(rho0)
     d.ntasks = len(tasks)
     for t, (key, op) in enumerate(tasks):

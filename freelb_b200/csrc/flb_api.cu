@@ -254,6 +254,12 @@ void build_params(flb_lattice* h) {
     if (mrt_conserved(k)) s = 0.0;
     p.s_over_norm[k] = s / double(mrt_norm(k));
   }
+  // one rate for all moments outside the conserved and shear sets: the
+  // two-rate form of the FP16S MRT collision
+  p.mrt_sg = float(d.mrt_rates[1]);
+  for (int k = 0; k < Q; ++k)
+    if (!mrt_conserved(k) && !mrt_shear(k) && d.mrt_rates[k] != d.mrt_rates[1]) p.mrt_sg = 0.0f;
+  if (!(p.mrt_sg > 0.0f)) p.mrt_sg = 0.0f;
   for (int i = 0; i < Q; ++i) {
     const double w = i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
     p.shift[i] = float(d.rho0 * w);
@@ -480,10 +486,18 @@ int pipe_prepare_t(flb_lattice* h) {
   return pipe_wide(h) ? pipe_prepare_w<MODEL, true>(h) : pipe_prepare_w<MODEL, false>(h);
 }
 
+// FP16S MRT with one rate for every non-conserved, non-shear moment runs the
+// two-rate kernels (MODEL_MRT2).
+bool fp16_mrt2(const flb_lattice* h) {
+  return h->desc.storage == FLB_STORAGE_FP16S && h->desc.model == FLB_MODEL_MRT &&
+         h->sp.mrt_sg != 0.0f;
+}
+
 int pipe_prepare(flb_lattice* h) {
   if (h->pipe_ctas > 0) return FLB_OK;
   switch (h->desc.model) {
-    case FLB_MODEL_MRT: return pipe_prepare_t<MODEL_MRT>(h);
+    case FLB_MODEL_MRT:
+      return fp16_mrt2(h) ? pipe_prepare_t<MODEL_MRT2>(h) : pipe_prepare_t<MODEL_MRT>(h);
     case FLB_MODEL_LES: return pipe_prepare_t<MODEL_LES>(h);
     default: return pipe_prepare_t<MODEL_BGK>(h);
   }
@@ -513,6 +527,8 @@ int tma_prepare(flb_lattice* h) {
   FLB_TRY((tma_attr<MODEL_BGK, 3, 4>()));
   FLB_TRY((tma_attr<MODEL_MRT, 5, 2>()));
   FLB_TRY((tma_attr<MODEL_MRT, 3, 4>()));
+  FLB_TRY((tma_attr<MODEL_MRT2, 5, 2>()));
+  FLB_TRY((tma_attr<MODEL_MRT2, 3, 4>()));
   FLB_TRY((tma_attr<MODEL_LES, 5, 2>()));
   FLB_TRY((tma_attr<MODEL_LES, 3, 4>()));
   h->tma_ready = true;
@@ -654,7 +670,15 @@ int launch_steps(flb_lattice* h, int nsteps, cudaStream_t st) {
     h->sp.dst = h->pops[h->cur ^ 1];
     switch (h->desc.model) {
       case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
-      case FLB_MODEL_MRT: launch_one_step<S, R, MODEL_MRT>(h, st); break;
+      case FLB_MODEL_MRT:
+        if constexpr (std::is_same<S, __half>::value) {
+          if (fp16_mrt2(h)) {
+            launch_one_step<S, R, MODEL_MRT2>(h, st);
+            break;
+          }
+        }
+        launch_one_step<S, R, MODEL_MRT>(h, st);
+        break;
       case FLB_MODEL_LES: launch_one_step<S, R, MODEL_LES>(h, st); break;
       default:
         if constexpr (!std::is_same<S, __half>::value)
@@ -679,7 +703,15 @@ int step_between(flb_lattice* h, const void* src, void* dst, cudaStream_t st) {
     using R = std::remove_pointer_t<decltype(rp)>;
     switch (h->desc.model) {
       case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
-      case FLB_MODEL_MRT: launch_one_step<S, R, MODEL_MRT>(h, st); break;
+      case FLB_MODEL_MRT:
+        if constexpr (std::is_same<S, __half>::value) {
+          if (fp16_mrt2(h)) {
+            launch_one_step<S, R, MODEL_MRT2>(h, st);
+            break;
+          }
+        }
+        launch_one_step<S, R, MODEL_MRT>(h, st);
+        break;
       case FLB_MODEL_LES: launch_one_step<S, R, MODEL_LES>(h, st); break;
       default:
         if constexpr (!std::is_same<S, __half>::value)

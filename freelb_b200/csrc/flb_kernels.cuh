@@ -56,6 +56,9 @@ struct StepParams {
   float scale, inv_scale;
   float rho0;         // FP16S: density of the shift
   int fp16_round;     // FP16S stores: 0 round to nearest, 1 stochastic (cvt.rs)
+  float mrt_sg;       // the one rate of every non-conserved, non-shear MRT
+                      // moment, or 0 when the rates differ (FP16S MRT then
+                      // runs the general form instead of MODEL_MRT2)
 };
 
 // First task whose key shares a bit with the flag (src/utils/tmp.h:283-309),
@@ -65,7 +68,12 @@ __device__ __forceinline__ int select_op(const StepParams& p, uint8_t flag) {
 }
 
 enum : int { OP_NONE = 0, OP_BULK = 1, OP_BB = 2, OP_MBB = 3, OP_FIELD_BGK = 4 };
-enum : int { MODEL_BGK = 0, MODEL_MRT = 1, MODEL_LES = 2, MODEL_BRINKMAN = 3 };
+enum : int { MODEL_BGK = 0, MODEL_MRT = 1, MODEL_LES = 2, MODEL_BRINKMAN = 3, MODEL_MRT2 = 4 };
+// MODEL_MRT2: the FP16S kernels' two-rate MRT form (every non-conserved,
+// non-shear moment at one rate), chosen on the host; everywhere else it is MRT.
+__host__ __device__ constexpr bool is_mrt(int model) {
+  return model == MODEL_MRT || model == MODEL_MRT2;
+}
 
 // The ops every model shares: bounce-back, moving wall, field-velocity BGK.
 template <typename R>

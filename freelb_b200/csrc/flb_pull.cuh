@@ -534,6 +534,73 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
   }
 }
 
+// k_i = 3 c_i . u of direction i (odd i; its pair partner i + 1 has -k_i)
+__device__ __forceinline__ float2 kdir2(int i, float2 k1, float2 k3, float2 k5) {
+  return i == 1 ? k1 : i == 3 ? k3 : i == 5 ? k5 : i == 7 ? add2(k1, k3) : i == 9 ? add2(k1, k5)
+       : i == 11 ? add2(k3, k5) : i == 13 ? sub2(k1, k3) : i == 15 ? sub2(k1, k5) : sub2(k3, k5);
+}
+
+// Two-rate MRT on deviations (pair form): every non-conserved moment outside
+// the shear set relaxes at s_g = p.mrt_sg, so M^-1 S M N = s_g N +
+// (omega - s_g) P N with P the projection on the five shear moments (the
+// conserved moments of N vanish up to FP32 rounding, as in the BGK form).  The
+// shear moments are even: the pair sums of N give them, and both members of a
+// pair get the same correction.  With E_i = S w_i (delta + rho (e_i +- k_i)):
+//   H'_i = (1 - s_g) H_i + s_g E_i - sum_shear M_ki mu_k,
+//   mu_k = (omega - s_g) / |M_k|^2 * sum_pairs M_ki (N_i + N_opp(i)).
+// Only the five moment sums live across the two passes over the pairs (the
+// pair terms are recomputed), which keeps it inside the step kernels'
+// register budget.  Explicit two-wide operations, as in mrt_deviation2.
+__device__ __forceinline__ void mrt_two_rate2(const StepParams& p, float2 (&H)[Q], float omega,
+                                              float2 rho, float2 delta, float2 q, float2 k1,
+                                              float2 k3, float2 k5) {
+  constexpr int SH[5] = {9, 11, 13, 14, 15};
+  const float s0 = p.scale * (1.0f / 3.0f), s1 = p.scale * (1.0f / 18.0f),
+              s2 = p.scale * (1.0f / 36.0f);
+  const float sg = p.mrt_sg;
+  float2 m[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) m[j] = p2(0.0f);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float sw = i < 7 ? s1 : s2;
+    const float2 k = kdir2(i, k1, k3, k5);
+    const float2 t = fma2(rho, fma2(mul2(p2(0.5f), k), k, q), delta);
+    const float2 a = fma2(p2(-2.0f * sw), t, add2(H[i], H[i + 1]));  // N_i + N_opp(i)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int c = mrt_m(SH[j], i);
+      if (c == 1) m[j] = add2(m[j], a);
+      else if (c == -1) m[j] = sub2(m[j], a);
+      else if (c != 0) m[j] = fma2(p2(float(c)), a, m[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 5; ++j) m[j] = mul2(m[j], p2((omega - sg) * (1.0f / float(mrt_norm_lit(SH[j])))));
+  const float2 keep = p2(1.0f - sg);
+  static_assert(mrt_m(9, 0) == 0 && mrt_m(11, 0) == 0 && mrt_m(13, 0) == 0 &&
+                    mrt_m(14, 0) == 0 && mrt_m(15, 0) == 0,
+                "shear moments leave the rest population alone");
+  H[0] = fma2(keep, H[0], mul2(p2(sg * s0), fma2(rho, q, delta)));
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float sw = sg * (i < 7 ? s1 : s2);
+    const float2 k = kdir2(i, k1, k3, k5);
+    const float2 t = fma2(rho, fma2(mul2(p2(0.5f), k), k, q), delta);
+    const float2 rk = mul2(rho, k);
+    float2 corr = p2(0.0f);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int c = mrt_m(SH[j], i);
+      if (c == 1) corr = add2(corr, m[j]);
+      else if (c == -1) corr = sub2(corr, m[j]);
+      else if (c != 0) corr = fma2(p2(float(c)), m[j], corr);
+    }
+    H[i] = sub2(fma2(keep, H[i], mul2(p2(sw), add2(t, rk))), corr);
+    H[i + 1] = sub2(fma2(keep, H[i + 1], mul2(p2(sw), sub2(t, rk))), corr);
+  }
+}
+
 // MRT on deviations for two cells at once (the pair form of bgk_deviation2):
 // the non-equilibrium part N = H - E in stored units, the 15 non-conserved
 // moments of N, their relaxation and the back-transform, every operation one
@@ -541,6 +608,7 @@ __device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, f
 // to the compiler), so each cell's result is the same whichever cell shares
 // its pair.  Every FP16S MRT bulk cell goes through it (a lone one on a
 // duplicated lane).
+template <int MODEL>
 __device__ __forceinline__ void mrt_deviation2(const StepParams& p, float2 (&H)[Q], float omega) {
   float2 sp[Q], df[Q];
 #pragma unroll
@@ -574,6 +642,10 @@ __device__ __forceinline__ void mrt_deviation2(const StepParams& p, float2 (&H)[
   const float s0 = p.scale * (1.0f / 3.0f), s1 = p.scale * (1.0f / 18.0f),
               s2 = p.scale * (1.0f / 36.0f);
   const float2 n0 = fma2(p2(-s0), fma2(rho, q, delta), H[0]);
+  if constexpr (MODEL == MODEL_MRT2) {  // host: p.mrt_sg != 0
+    mrt_two_rate2(p, H, omega, rho, delta, q, k1, k3, k5);
+    return;
+  }
   float2 a[9], b[9];
 #pragma unroll
   for (int i = 1; i < Q; i += 2) {
@@ -799,7 +871,7 @@ __device__ __forceinline__ void collide_dev32(const StepParams& p, int op, float
       float delta, rho, den, ux, uy, uz, N[Q];
       dev_moments(d, p.rho0, 0.0f, delta, rho, den, ux, uy, uz);
       dev_neq(d, delta, rho, ux, uy, uz, N);
-      if constexpr (MODEL == MODEL_MRT) {
+      if constexpr (is_mrt(MODEL)) {
         mrt_relax_neq(p, d, omega, N);
       } else if constexpr (MODEL == MODEL_LES) {
         les_relax_neq(p, d, omega, rho, N);
@@ -825,12 +897,12 @@ template <int MODEL>
 __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, float (&H)[Q],
                                                   long long cell, float omega) {
   if (op == OP_NONE) return;
-  if constexpr (MODEL == MODEL_MRT) {
+  if constexpr (is_mrt(MODEL)) {
     if (op == OP_BULK) {
       float2 H2[Q];
 #pragma unroll
       for (int i = 0; i < Q; ++i) H2[i] = p2(H[i]);
-      mrt_deviation2(p, H2, omega);
+      mrt_deviation2<MODEL>(p, H2, omega);
 #pragma unroll
       for (int i = 0; i < Q; ++i) H[i] = H2[i].x;
       return;
@@ -918,18 +990,18 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
     if (opa == OP_NONE && opb == OP_NONE) continue;
     // stochastic rounding is built for BGK and MRT (LES, instruction-bound,
     // keeps round to nearest and no trace of the other mode)
-    constexpr bool kSR = MODEL == MODEL_BGK || MODEL == MODEL_MRT;
+    constexpr bool kSR = MODEL == MODEL_BGK || is_mrt(MODEL);
     const bool sr = kSR && p.fp16_round;
     unsigned c = 0u;
     if (sr) c = sr_pair(hpart(h[0], k), hpart(h[1], k), hpart(h[9], k), hpart(h[18], k));
-    if ((MODEL == MODEL_BGK || MODEL == MODEL_MRT) && opa == OP_BULK && opb == OP_BULK) {
+    if ((MODEL == MODEL_BGK || is_mrt(MODEL)) && opa == OP_BULK && opb == OP_BULK) {
       float2 H2[Q];
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
         const unsigned q = hpart(h[i], k);
         H2[i] = __half22float2(*reinterpret_cast<const __half2*>(&q));
       }
-      if constexpr (MODEL == MODEL_MRT) mrt_deviation2(p, H2, omega);
+      if constexpr (is_mrt(MODEL)) mrt_deviation2<MODEL>(p, H2, omega);
       else bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
       if (sr) {
 #pragma unroll
@@ -1150,7 +1222,7 @@ template <typename S, int MODEL, int V>
 struct PullBounds {
   static constexpr int min_ctas =
       std::is_same<S, double>::value                          ? 1
-      : std::is_same<S, __half>::value && (MODEL == MODEL_BGK || MODEL == MODEL_MRT) ? 2
+      : std::is_same<S, __half>::value && (MODEL == MODEL_BGK || is_mrt(MODEL)) ? 2
       : (std::is_same<S, float>::value || std::is_same<S, dev32>::value) && V == 4 ? 2
                                                               : 3;
 };

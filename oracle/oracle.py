@@ -113,8 +113,9 @@ class Lattice:
         # omega = T(1)/T(RT) as in unit_converter.h:209
         d.omega = float(self.dtype.type(1) / tau_t)
         d.cs_smag = float(cs)
+        rates = [float(mrt_rate)] * 19 if np.isscalar(mrt_rate) else [float(r) for r in mrt_rate]
         for i in range(19):
-            d.mrt_s[i] = 0.0 if i in (0, 3, 5, 7) else float(mrt_rate)
+            d.mrt_s[i] = 0.0 if i in (0, 3, 5, 7) else rates[i]
         lut = task_lut(keys, ops)
         for v in range(256):
             d.op_lut[v] = int(lut[v])

@@ -16,6 +16,10 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 W32 = O.W.astype(np.float32).astype(np.float64)
+# MRT rates per moment (rho, e, eps, jx, qx, jy, qy, jz, qz, 3pxx, 3pixx, pww,
+# piww, pxy, pyz, pxz, mx, my, mz; shear entries are replaced by 1/tau): one
+# rate for every other moment runs the two-rate form, these the general form
+GENERAL_RATES = [0, 1.1, 1.3, 0, 1.25, 0, 1.25, 0, 1.25, 1, 1.4, 1, 1.4, 1, 1, 1, 1.5, 1.5, 1.5]
 
 
 def ulp16(x):
@@ -25,7 +29,7 @@ def ulp16(x):
     return 2.0 ** (e - 10)
 
 
-def one_step_errors(model, mode, shape=(32, 12, 12), seed=5):
+def one_step_errors(model, mode, shape=(32, 12, 12), seed=5, rates=1.2):
     """Stored deviations H = (f - w) 2^10 after one FP16S step from a random
     binary16 state, in ulps of the FP64 oracle's H from the same state."""
     nx, ny, nz = shape
@@ -37,14 +41,14 @@ def one_step_errors(model, mode, shape=(32, 12, 12), seed=5):
     f0 = (W32[:, None] + h0 / 1024.0).reshape(-1)
     flags = np.full(N, 2, dtype=np.uint8)
     lat = F.Lattice(nx, ny, nz, 0.56, storage="fp16s", model=model, smagorinsky=0.12,
-                    mrt_rate=1.2)
+                    mrt_rate=rates)
     lat.set_rounding(mode)
     lat.upload_flags(flags)
     lat.upload_pops(f0.astype(np.float32))
     lat.step(1)
     fd = lat.download_pops(np.float32).astype(np.float64).reshape(19, N)
     lat.close()
-    ref = O.Lattice(nx, ny, nz, flags, model=model, tau=0.56, cs=0.12, mrt_rate=1.2,
+    ref = O.Lattice(nx, ny, nz, flags, model=model, tau=0.56, cs=0.12, mrt_rate=rates,
                     dtype=np.float64)
     ref.pops[:] = f0
     ref.step(1)
@@ -54,16 +58,24 @@ def one_step_errors(model, mode, shape=(32, 12, 12), seed=5):
     return ((hd - hx) / ulp16(hx))[sel]
 
 
-@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+@pytest.mark.parametrize("model", ["bgk", "mrt", "mrt_general", "les"])
 def test_nearest_is_within_half_an_ulp(gpu_ok, model):
-    e = one_step_errors(model, "nearest")
+    """Also pins both FP16S MRT forms (two-rate and general) to the FP64
+    oracle: their FP32 arithmetic stays far inside half an ulp."""
+    if model == "mrt_general":
+        e = one_step_errors("mrt", "nearest", rates=GENERAL_RATES)
+    else:
+        e = one_step_errors(model, "nearest")
     assert e.size > 20000
     assert np.max(np.abs(e)) < 0.51, np.max(np.abs(e))
 
 
-@pytest.mark.parametrize("model", ["bgk", "mrt"])
+@pytest.mark.parametrize("model", ["bgk", "mrt", "mrt_general"])
 def test_stochastic_is_within_one_ulp_and_unbiased(gpu_ok, model):
-    e = one_step_errors(model, "stochastic")
+    if model == "mrt_general":
+        e = one_step_errors("mrt", "stochastic", rates=GENERAL_RATES)
+    else:
+        e = one_step_errors(model, "stochastic")
     assert e.size > 20000
     assert np.max(np.abs(e)) < 1.01, np.max(np.abs(e))
     away = np.mean(np.abs(e) > 0.51)  # rounded away from the nearest value
