@@ -551,6 +551,7 @@ def run_ours(args, rank, world, local_rank):
     # headline: 512^3 BGK FP32, launch shape from the autotuner
     htau = 3 * 0.1 * ni / 10000 + 0.5 if args.model == "les" else 0.53
     lat = F.cavity(ni, tau=htau, ulid=0.1, storage=args.storage, model=args.model)
+    lat.set_rounding(args.rounding)
     if args.launch:
         launch = tuple(int(v) for v in args.launch.split(","))
         lat.set_launch(*launch)
@@ -727,6 +728,8 @@ def main():
                     help="population storage of the headline run (profiling)")
     ap.add_argument("--model", default="bgk", choices=["bgk", "mrt", "les"],
                     help="collision model of the headline run (profiling; the headline is BGK)")
+    ap.add_argument("--rounding", default="default", choices=["default", "nearest", "stochastic"],
+                    help="FP16S rounding of the headline run (profiling)")
     ap.add_argument("--launch", default=None,
                     help="tile_y,ctas_per_sm,cells_per_thread for the headline run instead of "
                          "the autotuner (profiling)")
