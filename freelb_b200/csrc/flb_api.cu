@@ -486,18 +486,18 @@ int pipe_prepare_t(flb_lattice* h) {
   return pipe_wide(h) ? pipe_prepare_w<MODEL, true>(h) : pipe_prepare_w<MODEL, false>(h);
 }
 
-// FP16S MRT with one rate for every non-conserved, non-shear moment runs the
-// two-rate kernels (MODEL_MRT2).
-bool fp16_mrt2(const flb_lattice* h) {
-  return h->desc.storage == FLB_STORAGE_FP16S && h->desc.model == FLB_MODEL_MRT &&
-         h->sp.mrt_sg != 0.0f;
+// FP16S and FP32 MRT with one rate for every non-conserved, non-shear moment
+// run the two-rate kernels (MODEL_MRT2); FP32S and FP64 keep the general form.
+bool use_mrt2(const flb_lattice* h) {
+  return (h->desc.storage == FLB_STORAGE_FP16S || h->desc.storage == FLB_STORAGE_FP32) &&
+         h->desc.model == FLB_MODEL_MRT && h->sp.mrt_sg != 0.0f;
 }
 
 int pipe_prepare(flb_lattice* h) {
   if (h->pipe_ctas > 0) return FLB_OK;
   switch (h->desc.model) {
     case FLB_MODEL_MRT:
-      return fp16_mrt2(h) ? pipe_prepare_t<MODEL_MRT2>(h) : pipe_prepare_t<MODEL_MRT>(h);
+      return use_mrt2(h) ? pipe_prepare_t<MODEL_MRT2>(h) : pipe_prepare_t<MODEL_MRT>(h);
     case FLB_MODEL_LES: return pipe_prepare_t<MODEL_LES>(h);
     default: return pipe_prepare_t<MODEL_BGK>(h);
   }
@@ -671,8 +671,8 @@ int launch_steps(flb_lattice* h, int nsteps, cudaStream_t st) {
     switch (h->desc.model) {
       case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
       case FLB_MODEL_MRT:
-        if constexpr (std::is_same<S, __half>::value) {
-          if (fp16_mrt2(h)) {
+        if constexpr (std::is_same<S, __half>::value || std::is_same<S, float>::value) {
+          if (use_mrt2(h)) {
             launch_one_step<S, R, MODEL_MRT2>(h, st);
             break;
           }
@@ -704,8 +704,8 @@ int step_between(flb_lattice* h, const void* src, void* dst, cudaStream_t st) {
     switch (h->desc.model) {
       case FLB_MODEL_BGK: launch_one_step<S, R, MODEL_BGK>(h, st); break;
       case FLB_MODEL_MRT:
-        if constexpr (std::is_same<S, __half>::value) {
-          if (fp16_mrt2(h)) {
+        if constexpr (std::is_same<S, __half>::value || std::is_same<S, float>::value) {
+          if (use_mrt2(h)) {
             launch_one_step<S, R, MODEL_MRT2>(h, st);
             break;
           }

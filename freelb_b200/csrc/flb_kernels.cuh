@@ -57,8 +57,8 @@ struct StepParams {
   float rho0;         // FP16S: density of the shift
   int fp16_round;     // FP16S stores: 0 round to nearest, 1 stochastic (cvt.rs)
   float mrt_sg;       // the one rate of every non-conserved, non-shear MRT
-                      // moment, or 0 when the rates differ (FP16S MRT then
-                      // runs the general form instead of MODEL_MRT2)
+                      // moment, or 0 when the rates differ (MRT then runs
+                      // the general form instead of MODEL_MRT2)
 };
 
 // First task whose key shares a bit with the flag (src/utils/tmp.h:283-309),
@@ -69,8 +69,9 @@ __device__ __forceinline__ int select_op(const StepParams& p, uint8_t flag) {
 
 enum : int { OP_NONE = 0, OP_BULK = 1, OP_BB = 2, OP_MBB = 3, OP_FIELD_BGK = 4 };
 enum : int { MODEL_BGK = 0, MODEL_MRT = 1, MODEL_LES = 2, MODEL_BRINKMAN = 3, MODEL_MRT2 = 4 };
-// MODEL_MRT2: the FP16S kernels' two-rate MRT form (every non-conserved,
-// non-shear moment at one rate), chosen on the host; everywhere else it is MRT.
+// MODEL_MRT2: the two-rate MRT form (every non-conserved, non-shear moment at
+// one rate), chosen on the host for FP16S and FP32 storage; it is MRT in every
+// other respect.
 __host__ __device__ constexpr bool is_mrt(int model) {
   return model == MODEL_MRT || model == MODEL_MRT2;
 }
@@ -101,6 +102,8 @@ __device__ __forceinline__ void apply_op(const StepParams& p, int op, R* f, long
       smagorinsky_bgk<R>(f, R(1) / omega, R(p.cs_coeff));
     } else if constexpr (MODEL == MODEL_BRINKMAN) {
       bgk_brinkman<R>(f, omega, static_cast<const R*>(p.alpha)[cell]);
+    } else if constexpr (MODEL == MODEL_MRT2) {
+      mrt_two_rate<R>(f, omega, R(p.mrt_sg));
     } else {
       R s[Q];
 #pragma unroll

@@ -419,6 +419,49 @@ __device__ __forceinline__ void mrt_relax(R* f, R r0, const R (&a)[9], const R (
   }
 }
 
+// Two-rate MRT: every non-conserved moment outside the five (even) shear
+// moments relaxes at sg, so M^-1 S M n = sg n + (omega - sg) P n with n = f -
+// feq and P the projection on the shear moments, which the pair sums of n give
+// (both members of a pair get the same correction).  The same operator as mrt()
+// for such rate sets, with 5 moment sums instead of 15.
+template <typename R>
+__device__ __forceinline__ void mrt_two_rate(R* f, R omega, R sg) {
+  constexpr int SH[5] = {9, 11, 13, 14, 15};
+  R rho, ux, uy, uz, feq[Q];
+  rho_u(f, rho, ux, uy, uz);
+  feq2(feq, rho, ux, uy, uz);
+  R m[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) m[j] = R(0);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const R a = (f[i] - feq[i]) + (f[i + 1] - feq[i + 1]);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int c = mrt_m(SH[j], i);
+      if (c == 1) m[j] += a;
+      else if (c == -1) m[j] -= a;
+      else if (c != 0) m[j] += R(c) * a;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 5; ++j) m[j] *= (omega - sg) * (R(1) / R(mrt_norm_lit(SH[j])));
+  f[0] -= sg * (f[0] - feq[0]);
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    R corr = R(0);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int c = mrt_m(SH[j], i);
+      if (c == 1) corr += m[j];
+      else if (c == -1) corr -= m[j];
+      else if (c != 0) corr += R(c) * m[j];
+    }
+    f[i] -= sg * (f[i] - feq[i]) + corr;
+    f[i + 1] -= sg * (f[i + 1] - feq[i + 1]) + corr;
+  }
+}
+
 template <typename R>
 __device__ __forceinline__ void mrt(R* f, const R* s_over_norm) {
   R rho, ux, uy, uz, feq[Q];
