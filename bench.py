@@ -257,7 +257,7 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les
     taus = {"bgk": 0.53, "mrt": 0.53, "les": 3 * 0.1 * ni / 10000 + 0.5}
     for model, tau in ((m, taus[m]) for m in models):
         us = {}
-        other = {"mrt": "nearest", "bgk": "stochastic"}.get(model)
+        other = "nearest" if model == "mrt" else "stochastic"
         for storage in ("fp64", "fp32", "fp32s", "fp16s") + (("fp16s_" + other,) if other else ()):
             lat = F.cavity(ni, tau=tau, ulid=0.1, storage=storage.split("_")[0], model=model)
             lat.set_rounding(other if "_" in storage else "default")
@@ -627,6 +627,7 @@ def run_ours(args, rank, world, local_rank):
                                          ("fp16s", "mrt", 0.53, "nearest"),
                                          ("fp32", "les", les_tau, "default"),
                                          ("fp16s", "les", les_tau, "default"),
+                                         ("fp16s", "les", les_tau, "stochastic"),
                                          ("fp64", "bgk", 0.53, "default"),
                                          ("fp32s", "bgk", 0.53, "default")):
             ms, lch, vl = timed_cavity(F, torch, stream, ni, args.steps, 2, storage, model,
@@ -713,7 +714,36 @@ def run_ours(args, rank, world, local_rank):
                                 "sample": f"{CPU_BASELINE_STEPS} timed steps of the {ni}^3 cavity "
                                           f"on the reference FreeLB OpenMP path ({cpu['binary']})"}
     line.update(extras)
+    if extras:
+        line["summary"] = summary_of(line)
     print(json.dumps(compact(line)))
+
+
+def summary_of(line):
+    """The secondary figures in a few hundred characters, last on the line (a
+    log tail that cuts the line keeps them)."""
+    out = {}
+    v = line.get("variants", {})
+    out["glups"] = {"bgk": [line["value"], v.get("bgk_fp16s", {}).get("glups")],
+                    "mrt": [v.get("mrt_fp32", {}).get("glups"), v.get("mrt_fp16s", {}).get("glups")],
+                    "les": [v.get("les_fp32", {}).get("glups"), v.get("les_fp16s", {}).get("glups")],
+                    "order": "fp32, fp16s (default rounding)"}
+    out["roofline_frac_fp16s"] = {m: v.get(f"{m}_fp16s", {}).get("frac") for m in ("bgk", "mrt", "les")}
+    acc = line.get("accuracy", {}).get("models", {})
+    out["fp16s_rel_l2_u"] = {m: acc[m].get("fp16s_rel_l2_u") for m in acc}
+    ens = line.get("ensemble_128", {})
+    if ens:
+        out["ensemble_batched_vs_sequential"] = {
+            s: [ens[s]["batched_glups"], ens[s]["sequential_glups"]] for s in ("fp32", "fp16s")}
+    if "blocks_256" in line:
+        out["blocks_glups_stored"] = line["blocks_256"]["glups_stored"]
+    adj = line.get("adjoint_128", {}).get("fp32s")
+    if adj:
+        out["adjoint"] = {"backward_to_forward": adj["adjoint_to_forward_ratio"],
+                          "fd_rel_err_alpha_max": adj["fd_rel_err_alpha_max"]}
+    par = line.get("parity_256_vs_reference", {})
+    out["parity_pops_vs_reference"] = {m: par[m].get("pops") for m in par if isinstance(par[m], dict)}
+    return out
 
 
 def main():

@@ -276,10 +276,7 @@ void build_params(flb_lattice* h) {
   const int r = h->rounding == FLB_ROUND_DEFAULT
                     ? (d.model == FLB_MODEL_MRT ? FLB_ROUND_STOCHASTIC : FLB_ROUND_NEAREST)
                     : h->rounding;
-  p.fp16_round = d.storage == FLB_STORAGE_FP16S && r == FLB_ROUND_STOCHASTIC &&
-                         (d.model == FLB_MODEL_BGK || d.model == FLB_MODEL_MRT)
-                     ? 1
-                     : 0;
+  p.fp16_round = d.storage == FLB_STORAGE_FP16S && r == FLB_ROUND_STOCHASTIC ? 1 : 0;
 }
 
 // Cells per thread of the pull kernel (launch parameter; defaults are the
@@ -1499,9 +1496,6 @@ int flb_set_rounding(flb_lattice* h, int mode) {
   if (!h) return fail(FLB_ERR_INVALID, "null handle");
   if (mode != FLB_ROUND_DEFAULT && mode != FLB_ROUND_NEAREST && mode != FLB_ROUND_STOCHASTIC)
     return fail(FLB_ERR_INVALID, "rounding mode %d", mode);
-  if (mode == FLB_ROUND_STOCHASTIC && h->desc.storage == FLB_STORAGE_FP16S &&
-      h->desc.model != FLB_MODEL_BGK && h->desc.model != FLB_MODEL_MRT)
-    return fail(FLB_ERR_UNSUPPORTED, "stochastic FP16S rounding is built for BGK and MRT");
   h->rounding = mode;
   const StepParams keep = h->sp;
   build_params(h);

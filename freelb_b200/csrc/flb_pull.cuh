@@ -487,52 +487,6 @@ __device__ __forceinline__ void bgk_deviation2(float2 (&H)[Q], float omega, floa
   }
 }
 
-// Equilibrium of one cell in stored units, E_i = S (feq_i - w_i rho0)
-// = S w_i (delta + rho g_i), and the non-equilibrium part N_i = H_i - E_i =
-// S (f_i - feq_i), both without forming f_i (the deviation form above).  Every
-// product that meets an addition is either an explicit fmaf or rounded on its
-// own (__fmul_rn), so no contraction is left to the compiler and the result is
-// the same in every kernel this is inlined into.
-__device__ __forceinline__ void deviation_neq(const float (&H)[Q], float rho0, float scale,
-                                              float inv_scale, float& rho, float (&N)[Q]) {
-  float sp[Q], df[Q];
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    sp[i] = H[i] + H[i + 1];
-    df[i] = H[i] - H[i + 1];
-  }
-  const float sum = ((H[0] + sp[1]) + (sp[3] + sp[5])) + ((sp[7] + sp[9]) + (sp[11] + sp[13])) +
-                    (sp[15] + sp[17]);
-  const float mx = (df[1] + df[7]) + (df[9] + df[13]) + df[15];
-  const float my = (df[3] + df[7]) + (df[11] - df[13]) + df[17];
-  const float mz = (df[5] + df[9]) + (df[11] - df[15]) - df[17];
-  const float delta = sum * inv_scale;  // exact: inv_scale is a power of two
-  rho = rho0 + delta;
-  const float ir = __fdividef(inv_scale, rho);
-  const float ux = mx * ir, uy = my * ir, uz = mz * ir;
-  const float q = -1.5f * fmaf(ux, ux, fmaf(uy, uy, uz * uz));
-  const float k1 = __fmul_rn(3.0f, ux), k3 = __fmul_rn(3.0f, uy), k5 = __fmul_rn(3.0f, uz);
-  float k[Q];
-  k[1] = k1;
-  k[3] = k3;
-  k[5] = k5;
-  k[7] = k1 + k3;
-  k[9] = k1 + k5;
-  k[11] = k3 + k5;
-  k[13] = k1 - k3;
-  k[15] = k1 - k5;
-  k[17] = k3 - k5;
-  const float s0 = scale * (1.0f / 3.0f), s1 = scale * (1.0f / 18.0f),
-              s2 = scale * (1.0f / 36.0f);
-  N[0] = fmaf(-s0, fmaf(rho, q, delta), H[0]);
-#pragma unroll
-  for (int i = 1; i < Q; i += 2) {
-    const float sw = i < 7 ? s1 : s2;
-    const float e = fmaf(0.5f * k[i], k[i], q);
-    N[i] = fmaf(-sw, fmaf(rho, e + k[i], delta), H[i]);
-    N[i + 1] = fmaf(-sw, fmaf(rho, e - k[i], delta), H[i + 1]);
-  }
-}
 
 // k_i = 3 c_i . u of direction i (odd i; its pair partner i + 1 has -k_i)
 __device__ __forceinline__ float2 kdir2(int i, float2 k1, float2 k3, float2 k5) {
@@ -731,8 +685,8 @@ __device__ __forceinline__ void mrt_relax_neq(const StepParams& p, float (&H)[Q]
 
 // Smagorinsky BGK (collision::SmagorinskyBGK) on deviations: Pi^neq =
 // sum c c N / S, the effective rate from it, H <- H - omega_eff N, given the
-// cell's density and non-equilibrium part.  Products that meet additions are
-// explicit, as in deviation_neq.
+// cell's density and non-equilibrium part (the FP32S path).  Products that
+// meet additions are explicit, so no contraction is left to the compiler.
 __device__ __forceinline__ void les_relax_neq(const StepParams& p, float (&H)[Q], float omega,
                                               float rho, const float (&N)[Q]) {
   const float is = p.inv_scale;  // a power of two: the scaling is exact
@@ -759,10 +713,85 @@ __device__ __forceinline__ void les_relax_neq(const StepParams& p, float (&H)[Q]
   for (int i = 0; i < Q; ++i) H[i] = fmaf(-eomega, N[i], H[i]);
 }
 
-__device__ __forceinline__ void les_deviation(const StepParams& p, float (&H)[Q], float omega) {
-  float rho, N[Q];
-  deviation_neq(H, p.rho0, p.scale, p.inv_scale, rho, N);
-  les_relax_neq(p, H, omega, rho, N);
+
+// Smagorinsky BGK on deviations for two cells at once (the pair form of
+// bgk_deviation2).  Pi^neq needs no N array: with E the equilibrium part,
+// sum_i c_a c_b E_i / S = delta / 3 [a = b] + rho u_a u_b exactly for D3Q19,
+// so Pi^neq_ab = sum_i c_a c_b H_i / S - delta / 3 [a = b] - rho u_a u_b, and
+// c_a c_b is even, so the pair sums of H give it.  The effective rate
+// 1 / (tau + tau_t), tau_t = (sqrt(tau^2 + C |Pi| / rho) - tau) / 2
+// (collision::SmagorinskyBGK, src/lbm/collisionLES.h) is then a per-lane
+// scalar, and the update is BGK's H' = (1 - w) H + w E with w per lane.  The
+// square roots and reciprocals use the hardware approximations (MUFU, about
+// one FP32 ulp), far below the binary16 spacing the result is stored at; every
+// other operation is an explicit two-wide instruction, so each cell's result
+// is the same whichever cell shares its pair.
+__device__ __forceinline__ float les_rate(float nsq, float rho_inv, float rt_mol, float cs_coeff) {
+  const float norm = nsq > 0.0f ? __fmul_rn(nsq, rsqrtf(nsq)) : 0.0f;
+  const float t = __fmaf_rn(rt_mol, rt_mol, __fmul_rn(__fmul_rn(cs_coeff, rho_inv), norm));
+  const float rt_tur = __fmul_rn(0.5f, __fmul_rn(t, rsqrtf(t)) - rt_mol);
+  return __fdividef(1.0f, rt_mol + rt_tur);
+}
+
+__device__ __forceinline__ void les_deviation2(const StepParams& p, float2 (&H)[Q], float omega) {
+  float2 sp[Q], df[Q];
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    sp[i] = add2(H[i], H[i + 1]);
+    df[i] = sub2(H[i], H[i + 1]);
+  }
+  const float2 sum = add2(add2(add2(add2(H[0], sp[1]), add2(sp[3], sp[5])),
+                               add2(add2(sp[7], sp[9]), add2(sp[11], sp[13]))),
+                          add2(sp[15], sp[17]));
+  const float2 mx = add2(add2(add2(df[1], df[7]), add2(df[9], df[13])), df[15]);
+  const float2 my = add2(add2(add2(df[3], df[7]), sub2(df[11], df[13])), df[17]);
+  const float2 mz = sub2(add2(add2(df[5], df[9]), sub2(df[11], df[15])), df[17]);
+  const float is = p.inv_scale, scale = p.scale;
+  const float2 delta = mul2(sum, p2(is));
+  const float2 rho = add2(p2(p.rho0), delta);
+  const float2 ir = make_float2(__fdividef(is, rho.x), __fdividef(is, rho.y));  // 1 / (S rho)
+  const float2 ux = mul2(mx, ir), uy = mul2(my, ir), uz = mul2(mz, ir);
+  // Pi^neq in f units
+  const float2 d3 = mul2(delta, p2(1.0f / 3.0f));
+  const float2 rux = mul2(rho, ux), ruy = mul2(rho, uy);
+  const float2 pxx = sub2(fma2(add2(add2(add2(sp[1], sp[7]), add2(sp[9], sp[13])), sp[15]), p2(is),
+                              mul2(p2(-1.0f), d3)), mul2(rux, ux));
+  const float2 pyy = sub2(fma2(add2(add2(add2(sp[3], sp[7]), add2(sp[11], sp[13])), sp[17]), p2(is),
+                              mul2(p2(-1.0f), d3)), mul2(ruy, uy));
+  const float2 pzz = sub2(fma2(add2(add2(add2(sp[5], sp[9]), add2(sp[11], sp[15])), sp[17]), p2(is),
+                              mul2(p2(-1.0f), d3)), mul2(mul2(rho, uz), uz));
+  const float2 pxy = sub2(mul2(sub2(sp[7], sp[13]), p2(is)), mul2(rux, uy));
+  const float2 pxz = sub2(mul2(sub2(sp[9], sp[15]), p2(is)), mul2(rux, uz));
+  const float2 pyz = sub2(mul2(sub2(sp[11], sp[17]), p2(is)), mul2(ruy, uz));
+  float2 nsq = mul2(pxx, pxx);
+  nsq = fma2(mul2(pxy, pxy), p2(2.0f), nsq);
+  nsq = fma2(mul2(pxz, pxz), p2(2.0f), nsq);
+  nsq = fma2(pyy, pyy, nsq);
+  nsq = fma2(mul2(pyz, pyz), p2(2.0f), nsq);
+  nsq = fma2(pzz, pzz, nsq);
+  const float rt_mol = __fdividef(1.0f, omega);
+  const float csc = float(p.cs_coeff);
+  const float2 w = make_float2(les_rate(nsq.x, __fmul_rn(ir.x, scale), rt_mol, csc),
+                               les_rate(nsq.y, __fmul_rn(ir.y, scale), rt_mol, csc));
+  // BGK update with the per-lane rate w (bgk_deviation2's form)
+  const float2 q = mul2(p2(-1.5f), fma2(ux, ux, fma2(uy, uy, mul2(uz, uz))));
+  const float2 c1 = sub2(p2(1.0f), w);
+  const float2 W0 = mul2(w, p2(scale * (1.0f / 3.0f)));
+  const float2 W1 = mul2(w, p2(scale * (1.0f / 18.0f)));
+  const float2 W2 = mul2(w, p2(scale * (1.0f / 36.0f)));
+  const float2 d0 = mul2(W0, delta), d1 = mul2(W1, delta), d2 = mul2(W2, delta);
+  const float2 r0 = mul2(W0, rho), r1 = mul2(W1, rho), r2 = mul2(W2, rho);
+  const float2 k1 = mul2(p2(3.0f), ux), k3 = mul2(p2(3.0f), uy), k5 = mul2(p2(3.0f), uz);
+  H[0] = fma2(r0, q, fma2(c1, H[0], d0));
+#pragma unroll
+  for (int i = 1; i < Q; i += 2) {
+    const float2 dw = i < 7 ? d1 : d2;
+    const float2 rw = i < 7 ? r1 : r2;
+    const float2 k = kdir2(i, k1, k3, k5);
+    const float2 e = fma2(mul2(p2(0.5f), k), k, q);
+    H[i] = fma2(rw, add2(e, k), fma2(c1, H[i], dw));
+    H[i + 1] = fma2(rw, sub2(e, k), fma2(c1, H[i + 1], dw));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -910,7 +939,12 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
   }
   if constexpr (MODEL == MODEL_LES) {
     if (op == OP_BULK) {
-      les_deviation(p, H, omega);
+      float2 H2[Q];
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H2[i] = p2(H[i]);
+      les_deviation2(p, H2, omega);
+#pragma unroll
+      for (int i = 0; i < Q; ++i) H[i] = H2[i].x;
       return;
     }
   }
@@ -988,13 +1022,13 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
   for (int k = 0; k < V; k += 2) {
     const int opa = select_op(p, fl[k]), opb = select_op(p, fl[k + 1]);
     if (opa == OP_NONE && opb == OP_NONE) continue;
-    // stochastic rounding is built for BGK and MRT (LES, instruction-bound,
-    // keeps round to nearest and no trace of the other mode)
-    constexpr bool kSR = MODEL == MODEL_BGK || is_mrt(MODEL);
+    // stochastic rounding: every FP16S model (FP16S has no Brinkman kernels)
+    constexpr bool kSR = MODEL != MODEL_BRINKMAN;
     const bool sr = kSR && p.fp16_round;
     unsigned c = 0u;
     if (sr) c = sr_pair(hpart(h[0], k), hpart(h[1], k), hpart(h[9], k), hpart(h[18], k));
-    if ((MODEL == MODEL_BGK || is_mrt(MODEL)) && opa == OP_BULK && opb == OP_BULK) {
+    if ((MODEL == MODEL_BGK || is_mrt(MODEL) || MODEL == MODEL_LES) && opa == OP_BULK &&
+        opb == OP_BULK) {
       float2 H2[Q];
 #pragma unroll
       for (int i = 0; i < Q; ++i) {
@@ -1002,6 +1036,7 @@ __device__ __forceinline__ void collide_half(const StepParams& p, float omega, l
         H2[i] = __half22float2(*reinterpret_cast<const __half2*>(&q));
       }
       if constexpr (is_mrt(MODEL)) mrt_deviation2<MODEL>(p, H2, omega);
+      else if constexpr (MODEL == MODEL_LES) les_deviation2(p, H2, omega);
       else bgk_deviation2(H2, omega, p.rho0, p.scale, p.inv_scale);
       if (sr) {
 #pragma unroll
@@ -1215,14 +1250,15 @@ __device__ __forceinline__ bool chunk_coords(const Geom& g, long long q, int& x0
 // only padding lanes idle.  Grid: ceil(chunks / blockDim.x) CTAs.
 // Minimum resident 256-thread CTAs per SM asked of the compiler, i.e. the
 // register cap: 3 (85 registers, 24 warps per SM) for the FP32 kernels at 2
-// cells per thread and the FP16S LES kernel, 2 (128 registers) for FP16S BGK
-// and MRT (their two-wide pair code spills badly at 85) and FP32 at 4 cells
-// per thread; FP64 is left free.  Measured at 512^3 against the other caps.
+// cells per thread, 2 (128 registers) for the FP16S kernels (their two-wide
+// pair code spills badly at 85: LES 1.1 KB at 4 cells per thread) and FP32 at
+// 4 cells per thread; FP64 is left free.  Measured at 512^3 against the other
+// caps.
 template <typename S, int MODEL, int V>
 struct PullBounds {
   static constexpr int min_ctas =
       std::is_same<S, double>::value                          ? 1
-      : std::is_same<S, __half>::value && (MODEL == MODEL_BGK || is_mrt(MODEL)) ? 2
+      : std::is_same<S, __half>::value ? 2
       : (std::is_same<S, float>::value || std::is_same<S, dev32>::value) && V == 4 ? 2
                                                               : 3;
 };

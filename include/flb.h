@@ -344,10 +344,8 @@ FLB_API int flb_device_status(flb_lattice* lat, void* stream);
  * the flow changes slowly, and in MRT that error accumulates (the 512^3 cavity
  * ends 1.2e-3 from FP64 after 2000 steps, 3.7e-4 with stochastic rounding).
  * FLB_ROUND_DEFAULT (the default) is stochastic for MRT and round to nearest
- * otherwise.  Stochastic rounding is built for the BGK and MRT step kernels
- * (FLB_ERR_UNSUPPORTED for an FP16S LES or Brinkman handle, which always
- * round to nearest); other storages ignore the mode.  flb_get_rounding
- * returns the mode in effect (NEAREST or STOCHASTIC). */
+ * otherwise; other storages ignore the mode.  flb_get_rounding returns the
+ * mode in effect (NEAREST or STOCHASTIC). */
 #define FLB_ROUND_DEFAULT (-1)
 #define FLB_ROUND_NEAREST 0
 #define FLB_ROUND_STOCHASTIC 1

@@ -4,7 +4,7 @@ the same binary16 state.  Round to nearest stays within half a unit in the last
 place (ulp) of every stored deviation; stochastic rounding stays within one ulp,
 rounds away from the nearest value for about a quarter of them, and is
 unbiased (mean error far below the ulp).  The mode is per handle, defaults to
-stochastic for MRT only, is built for BGK and MRT, and both modes are
+stochastic for MRT only, and both modes are
 deterministic (the random bits come from the cell's own inputs)."""
 import numpy as np
 import pytest
@@ -70,7 +70,7 @@ def test_nearest_is_within_half_an_ulp(gpu_ok, model):
     assert np.max(np.abs(e)) < 0.51, np.max(np.abs(e))
 
 
-@pytest.mark.parametrize("model", ["bgk", "mrt", "mrt_general"])
+@pytest.mark.parametrize("model", ["bgk", "mrt", "mrt_general", "les"])
 def test_stochastic_is_within_one_ulp_and_unbiased(gpu_ok, model):
     if model == "mrt_general":
         e = one_step_errors("mrt", "stochastic", rates=GENERAL_RATES)
@@ -96,13 +96,11 @@ def test_modes_and_defaults(gpu_ok):
     with pytest.raises(F.FlbError):
         C.call("flb_set_rounding", lat._h, 7)
     les = F.cavity(10, storage="fp16s", model="les")
-    with pytest.raises(F.FlbError) as e:  # built for BGK and MRT only
-        les.set_rounding("stochastic")
-    assert e.value.code == -6
-    assert les.rounding() == "nearest"
+    les.set_rounding("stochastic")
+    assert les.rounding() == "stochastic"
 
 
-@pytest.mark.parametrize("model", ["bgk", "mrt"])
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
 def test_stochastic_runs_are_reproducible_and_differ_from_nearest(gpu_ok, model):
     """The random bits are a function of the state: two runs give the same
     bits, CUDA-graph replay gives the plain launches' bits, and the two modes

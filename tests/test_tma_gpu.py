@@ -31,8 +31,6 @@ def pair(make, steps, mode, rounding="default"):
 @pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
 @pytest.mark.parametrize("ni", [22, 30, 62])
 def test_tma_equals_direct_kernel_on_cavity(gpu_ok, model, ni, mode, rounding):
-    if model == "les" and rounding == "stochastic":
-        pytest.skip("LES rounds to nearest only")
     a, b = pair(lambda: F.cavity(ni, tau=0.55, storage="fp16s", model=model), 25, mode,
                 rounding)
     assert np.array_equal(a.download_pops(), b.download_pops())
@@ -64,7 +62,7 @@ def test_tma_equals_direct_kernel_on_random_flags(gpu_ok, model, dims):
         lat.upload_field("u", u)
         return lat
 
-    for rounding in ("nearest", "stochastic") if model != "les" else ("nearest",):
+    for rounding in ("nearest", "stochastic"):
         a, b = pair(make, 9, -2, rounding)
         assert np.array_equal(a.download_pops(), b.download_pops())
 
