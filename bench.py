@@ -705,6 +705,7 @@ def run_ours(args, rank, world, local_rank):
                 "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                 "job": "flags + VELOCITY in (pinned host), K steps, RHO + VELOCITY out"},
         "gpu_launches": args.steps,
+        "nonvoid_glups": ni ** 3 * args.steps * world / (ms32 / 1e3) / 1e9,
         "clocks": clocks,
         "nonfinite": bad32,
     }

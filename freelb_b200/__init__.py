@@ -192,6 +192,21 @@ class Lattice:
         """Bound of one device-side wait of the bulk-copy kernel (seconds)."""
         C.call("flb_set_wait_limit", self._h, float(seconds))
 
+    def snapshot_bytes(self):
+        n = ctypes.c_size_t()
+        C.call("flb_snapshot_bytes", self._h, ctypes.byref(n))
+        return int(n.value)
+
+    def snapshot_save(self, ptr, cap, stream=None):
+        """Copy the state (header + populations) to the buffer at address
+        `ptr` (device or host) of `cap` bytes."""
+        C.call("flb_snapshot_save", self._h, ctypes.c_void_p(ptr), ctypes.c_size_t(cap),
+               _stream(stream))
+
+    def snapshot_restore(self, ptr, nbytes, stream=None):
+        C.call("flb_snapshot_restore", self._h, ctypes.c_void_p(ptr), ctypes.c_size_t(nbytes),
+               _stream(stream))
+
     def set_rounding(self, mode):
         """Rounding of FP16S stores: "nearest", "stochastic" or "default"
         (stochastic for MRT, nearest otherwise)."""

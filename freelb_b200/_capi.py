@@ -96,6 +96,9 @@ SIGNATURES = {
     "flb_device_status": [_P, _P],
     "flb_test_withhold_tile": [_P, ctypes.c_longlong],
     "flb_set_rounding": [_P, _I],
+    "flb_snapshot_bytes": [_P, ctypes.POINTER(ctypes.c_size_t)],
+    "flb_snapshot_save": [_P, _P, ctypes.c_size_t, _P],
+    "flb_snapshot_restore": [_P, _P, ctypes.c_size_t, _P],
     "flb_get_rounding": [_P, ctypes.POINTER(_I)],
     "flb_autotune": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)],

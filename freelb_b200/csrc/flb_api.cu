@@ -1726,6 +1726,86 @@ int flb_check_finite(flb_lattice* h, uint64_t* bad, void* stream) {
   return FLB_OK;
 }
 
+// Snapshots: a 64-byte header, then the populations of every block in the
+// device layout (padded rows, the post-collision convention), as stored.
+namespace {
+struct SnapHeader {
+  char magic[8];        // "FLBSNAP1"
+  long long nbytes;     // population bytes after the header
+  long long dstride;    // elements per population array
+  int storage, nblocks;
+  unsigned long long geom;  // hash of the block shapes and origins
+  long long reserved[3];
+};
+static_assert(sizeof(SnapHeader) == 64, "snapshot header");
+
+unsigned long long geom_hash(const flb_lattice* h) {
+  unsigned long long x = 1469598103934665603ULL;  // FNV-1a over the block table
+  auto mix = [&](long long v) {
+    for (int b = 0; b < 8; ++b) {
+      x ^= (unsigned long long)(v >> (8 * b)) & 0xffULL;
+      x *= 1099511628211ULL;
+    }
+  };
+  for (const HostBlock& b : h->blocks) {
+    mix(b.L.nx); mix(b.L.ny); mix(b.L.nz); mix(b.ox); mix(b.oy); mix(b.oz); mix(b.base);
+  }
+  return x;
+}
+
+SnapHeader snap_header(const flb_lattice* h) {
+  SnapHeader hd{};
+  std::memcpy(hd.magic, "FLBSNAP1", 8);
+  hd.nbytes = (long long)Q * h->dstride * h->elem_bytes;
+  hd.dstride = h->dstride;
+  hd.storage = h->desc.storage;
+  hd.nblocks = int(h->blocks.size());
+  hd.geom = geom_hash(h);
+  return hd;
+}
+}  // namespace
+
+int flb_snapshot_bytes(const flb_lattice* h, size_t* bytes) {
+  if (!h || !bytes) return fail(FLB_ERR_INVALID, "null argument");
+  *bytes = sizeof(SnapHeader) + size_t(Q) * size_t(h->dstride) * h->elem_bytes;
+  return FLB_OK;
+}
+
+int flb_snapshot_save(flb_lattice* h, void* dst, size_t cap, void* stream) {
+  if (!h || !dst) return fail(FLB_ERR_INVALID, "null argument");
+  const SnapHeader hd = snap_header(h);
+  if (cap < sizeof hd + size_t(hd.nbytes))
+    return fail(FLB_ERR_INVALID, "snapshot buffer of %zu bytes < %zu", cap,
+                sizeof hd + size_t(hd.nbytes));
+  cudaStream_t st = as_stream(stream);
+  char* d = static_cast<char*>(dst);
+  // the header leaves host memory before cudaMemcpyAsync returns (pageable
+  // source); the populations follow on the stream
+  FLB_CUDA(cudaMemcpyAsync(d, &hd, sizeof hd, cudaMemcpyDefault, st));
+  FLB_CUDA(cudaMemcpyAsync(d + sizeof hd, h->pops[h->cur], size_t(hd.nbytes), cudaMemcpyDefault,
+                           st));
+  return FLB_OK;
+}
+
+int flb_snapshot_restore(flb_lattice* h, const void* src, size_t bytes, void* stream) {
+  if (!h || !src) return fail(FLB_ERR_INVALID, "null argument");
+  const SnapHeader want = snap_header(h);
+  if (bytes < sizeof want + size_t(want.nbytes))
+    return fail(FLB_ERR_INVALID, "snapshot of %zu bytes < %zu", bytes,
+                sizeof want + size_t(want.nbytes));
+  cudaStream_t st = as_stream(stream);
+  SnapHeader got{};
+  FLB_CUDA(cudaMemcpyAsync(&got, src, sizeof got, cudaMemcpyDefault, st));
+  FLB_CUDA(cudaStreamSynchronize(st));
+  if (std::memcmp(got.magic, want.magic, 8) != 0) return fail(FLB_ERR_INVALID, "not a snapshot");
+  if (got.nbytes != want.nbytes || got.dstride != want.dstride || got.storage != want.storage ||
+      got.nblocks != want.nblocks || got.geom != want.geom)
+    return fail(FLB_ERR_INVALID, "snapshot of another lattice (storage, blocks or shape)");
+  FLB_CUDA(cudaMemcpyAsync(h->pops[h->cur], static_cast<const char*>(src) + sizeof got,
+                           size_t(want.nbytes), cudaMemcpyDefault, st));
+  return FLB_OK;
+}
+
 int flb_get_layout(const flb_lattice* h, flb_layout* layout) {
   if (!h || !layout) return fail(FLB_ERR_INVALID, "null argument");
   const HostBlock& b = h->blocks[0];

@@ -334,6 +334,21 @@ FLB_API int flb_get_launch(const flb_lattice* lat, int* tile_y, int* ctas_per_sm
  * recorded code (which it clears). */
 FLB_API int flb_set_wait_limit(flb_lattice* lat, double seconds);
 FLB_API int flb_device_status(flb_lattice* lat, void* stream);
+/* Population snapshots (checkpoint / resume; no reference counterpart: FreeLB
+ * only writes VTK output and never reads populations back).  A snapshot is a
+ * 64-byte header followed by the populations of every block in the device
+ * layout, exactly as stored, so a restored handle continues bit for bit.
+ * flb_snapshot_bytes gives its size.  flb_snapshot_save copies the current
+ * state into `dst` (device memory, or host memory: pinned for an asynchronous
+ * copy), ordered on `stream`; `dst` must stay valid until the stream reaches
+ * it.  flb_snapshot_restore checks the header (synchronising `stream` for
+ * it) and copies the populations back: FLB_ERR_INVALID for a buffer that is
+ * not a snapshot, too short, or taken from a handle of another storage or
+ * block geometry.  Flags and fields are inputs and are not part of it. */
+FLB_API int flb_snapshot_bytes(const flb_lattice* lat, size_t* bytes);
+FLB_API int flb_snapshot_save(flb_lattice* lat, void* dst, size_t cap, void* stream);
+FLB_API int flb_snapshot_restore(flb_lattice* lat, const void* src, size_t bytes, void* stream);
+
 /* Rounding of FP16S stores (no reference counterpart: the reference stores
  * populations in T).  FLB_ROUND_NEAREST rounds every stored deviation to the
  * nearest binary16 value; FLB_ROUND_STOCHASTIC rounds it up or down with the
