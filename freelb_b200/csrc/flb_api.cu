@@ -123,6 +123,7 @@ struct flb_lattice {
   long long withhold = -1; // failure-detection test hook (flb_test_withhold_tile)
   int vec = 0;  // cells per thread of the step kernel; 0 = storage default
   int rounding = FLB_ROUND_DEFAULT;  // FP16S stores (flb_set_rounding)
+  alignas(8) char snap_hdr[64] = {};  // source of the snapshot header copies
   // CUDA graphs of the two-step cycle, one per starting buffer parity
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   // Brinkman porosity (FLB_FIELD_ALPHA), arithmetic type
@@ -1779,9 +1780,11 @@ int flb_snapshot_save(flb_lattice* h, void* dst, size_t cap, void* stream) {
                 sizeof hd + size_t(hd.nbytes));
   cudaStream_t st = as_stream(stream);
   char* d = static_cast<char*>(dst);
-  // the header leaves host memory before cudaMemcpyAsync returns (pageable
-  // source); the populations follow on the stream
-  FLB_CUDA(cudaMemcpyAsync(d, &hd, sizeof hd, cudaMemcpyDefault, st));
+  // the header is copied from the handle, which outlives the stream's copy
+  // (every header of a handle is the same bytes); the populations follow
+  static_assert(sizeof hd == sizeof h->snap_hdr, "snapshot header size");
+  std::memcpy(h->snap_hdr, &hd, sizeof hd);
+  FLB_CUDA(cudaMemcpyAsync(d, h->snap_hdr, sizeof hd, cudaMemcpyDefault, st));
   FLB_CUDA(cudaMemcpyAsync(d + sizeof hd, h->pops[h->cur], size_t(hd.nbytes), cudaMemcpyDefault,
                            st));
   return FLB_OK;

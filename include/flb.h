@@ -353,11 +353,11 @@ FLB_API int flb_snapshot_restore(flb_lattice* lat, const void* src, size_t bytes
  * populations in T).  FLB_ROUND_NEAREST rounds every stored deviation to the
  * nearest binary16 value; FLB_ROUND_STOCHASTIC rounds it up or down with the
  * probabilities that make the stored value exact on average (the sm_100a
- * cvt.rs conversion; the random bits come from a hash of the cell's own
- * post-collision values, so runs are reproducible and every kernel gives the
- * same bits).  Round to nearest makes the same error step after step where
- * the flow changes slowly, and in MRT that error accumulates (the 512^3 cavity
- * ends 1.2e-3 from FP64 after 2000 steps, 3.7e-4 with stochastic rounding).
+ * cvt.rs conversion; the random bits come from a hash of binary16 values the
+ * cell pulled, so runs are reproducible and every kernel gives the same
+ * bits).  Round to nearest can make the same error step after step where the
+ * flow changes slowly, and in MRT that error accumulates (the 512^3 cavity
+ * ends 1.17e-3 from FP64 after 2000 steps, 2.2e-4 with stochastic rounding).
  * FLB_ROUND_DEFAULT (the default) is stochastic for MRT and round to nearest
  * otherwise; other storages ignore the mode.  flb_get_rounding returns the
  * mode in effect (NEAREST or STOCHASTIC). */
