@@ -47,16 +47,17 @@ def test_blocks_match_reference_multiblock_golden(gpu_ok, name):
         assert np.array_equal(lat.download_flags(block=k), g[f"flags_b{k}"])
 
 
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
 @pytest.mark.parametrize("tile_y,ctas,vec", [(8, 0, 4), (2, 8, 2), (1, 0, 2), (4, 16, 4)])
-def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas, vec):
+def test_blocks_vs_single_block_bitwise_on_fluid(gpu_ok, tile_y, ctas, vec, model):
     """Uneven blocks with device halos reproduce the single-block run exactly on
-    fluid cells, for every launch shape."""
+    fluid cells, for every launch shape and model (MRT in its two-rate form)."""
     ni = 40
     blocks = G.uneven_blocks(ni, edges=(8, 12, 16), seed=5)
-    lat = gpu_blocks(ni, blocks, "fp32")
+    lat = gpu_blocks(ni, blocks, "fp32", model=model)
     lat.set_launch(tile_y, ctas, vec)
     lat.step(40)
-    one = F.cavity(ni)
+    one = F.cavity(ni, model=model)
     one.step(40)
     n = ni + 2
     P = one.download_pops().reshape(19, n, n, n)
