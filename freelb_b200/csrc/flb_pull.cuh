@@ -973,9 +973,9 @@ __device__ __forceinline__ void collide_deviation(const StepParams& p, int op, f
 // fraction of the low half, bits [28:16] that of the high half.  Round to
 // nearest can make the same error step after step where the flow changes
 // slowly, and that error adds up: MRT FP16S on the 512^3 cavity drifts
-// linearly to a velocity error of 1.2e-3 against FP64 after 2000 steps (BGK
-// stays at 3.2e-4; its modes of rate 1/tau ~ 1.9 flip sign every step, MRT's
-// other rates of 1.2 barely do), and stochastic rounding removes the drift.
+// linearly to a velocity error of 1.2e-3 against FP64 after 2000 steps, while
+// BGK, and MRT with every rate at 1/tau, stay at 3.2e-4 (so the drift comes
+// with MRT's other rates of 1.2); stochastic rounding removes it (2.2e-4).
 // The random fraction of a cell comes from a hash of four of the binary16
 // values it pulled (directions 0, 1, 9, 18), XORed with a per-direction key
 // that has the same 13 bits in both fields.  Those inputs are the same bits in
