@@ -162,7 +162,7 @@ def test_autotune_keeps_results_exact(gpu_ok, storage):
     a = F.cavity(36, storage=storage)
     b = F.cavity(36, storage=storage)
     (ty, c, v), ms, taken = a.autotune(trial_steps=2)
-    assert ty in (1, 2, 4, 8) and c in (-1, 0, 8, 16, 32) and ms > 0 and taken > 0
+    assert ty in (1, 2, 4, 8) and c in (-3, -2, -1, 0, 8, 16, 32) and ms > 0 and taken > 0
     assert c >= 0 or storage == "fp16s"
     assert v in ((1, 2) if storage == "fp64" else (2, 4))
     assert a.get_launch() == (ty, c, v)
@@ -194,19 +194,24 @@ def test_every_vector_width_matches_oracle(gpu_ok, storage, vec):
     assert rel_maxnorm(lat.download_pops(), ref.pops) < tol
 
 
-@pytest.mark.parametrize("storage,widths", [("fp32", (2, 4)), ("fp16s", (2, 4)), ("fp64", (1, 2))])
+@pytest.mark.parametrize("model", ["bgk", "mrt", "les"])
+@pytest.mark.parametrize("storage,widths", [("fp32", (2, 4)), ("fp16s", (2, 4)), ("fp64", (1, 2)),
+                                            ("fp32s", (2, 4))])
 @pytest.mark.parametrize("ni", [21, 30])
-def test_vector_widths_are_bitwise_equal(gpu_ok, storage, widths, ni):
+def test_vector_widths_are_bitwise_equal(gpu_ok, storage, widths, ni, model):
     """Every cell's update is the same function of its 19 sources whatever the
-    cells per thread, so the vector widths agree bit for bit (ragged rows and
-    row ends included)."""
+    cells per thread or launch shape (direct, persistent tile kernel), so they
+    agree bit for bit (ragged rows and row ends included): the autotuner's pick
+    never changes a result."""
     out = []
     for v in widths:
-        lat = F.cavity(ni, tau=0.55, storage=storage)
-        lat.set_launch(2, 0, v)
-        lat.step(25)
-        out.append(lat.download_pops())
-    assert np.array_equal(out[0], out[1])
+        for shape in ((2, 0, v), (8, 16, v)):
+            lat = F.cavity(ni, tau=0.55, storage=storage, model=model)
+            lat.set_launch(*shape)
+            lat.step(25)
+            out.append(lat.download_pops())
+    for o in out[1:]:
+        assert np.array_equal(out[0], o)
 
 
 @pytest.mark.parametrize("storage,tol", [("fp64", 1e-12), ("fp32", 1e-5), ("fp16s", 2e-3)])
