@@ -720,7 +720,7 @@ __device__ __forceinline__ void les_relax_neq(const StepParams& p, float (&H)[Q]
 // so Pi^neq_ab = sum_i c_a c_b H_i / S - delta / 3 [a = b] - rho u_a u_b, and
 // c_a c_b is even, so the pair sums of H give it.  The effective rate
 // 1 / (tau + tau_t), tau_t = (sqrt(tau^2 + C |Pi| / rho) - tau) / 2
-// (collision::SmagorinskyBGK, src/lbm/collisionLES.h) is then a per-lane
+// (collision::SmagorinskyBGK, src/lbm/collisionLES.h:36-62) is then a per-lane
 // scalar, and the update is BGK's H' = (1 - w) H + w E with w per lane.  The
 // square roots and reciprocals use the hardware approximations (MUFU, about
 // one FP32 ulp), far below the binary16 spacing the result is stored at; every
