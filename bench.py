@@ -238,10 +238,15 @@ def round_once_fp16s(pops):
     (direction by direction, in 16M-cell pieces, so a 512^3 lattice needs no
     second full-size host array)."""
     p = pops.reshape(19, -1)
+    out_of_range = 0  # |f - w| * 2^10 beyond binary16 (FP16S storage would hold inf there)
     for i, wi in enumerate(W19):
         for s in range(0, p.shape[1], 1 << 24):
             seg = p[i, s:s + (1 << 24)]
-            seg[:] = ((seg - wi) * 1024.0).astype(np.float16).astype(np.float64) / 1024.0 + wi
+            d = (seg - wi) * 1024.0
+            out_of_range += int(np.count_nonzero(~(np.abs(d) <= 65504.0)))
+            with np.errstate(over="ignore", invalid="ignore"):
+                seg[:] = d.astype(np.float16).astype(np.float64) / 1024.0 + wi
+    return out_of_range
 
 
 def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les")):
@@ -276,13 +281,15 @@ def accuracy_block(F, ni, steps, keep_bgk_fp32=False, models=("bgk", "mrt", "les
         lat = F.cavity(ni, tau=tau, ulid=0.1, storage="fp64", model=model)
         lat.step(steps // 2)
         pops = lat.download_pops(np.float64)
-        round_once_fp16s(pops)
+        beyond = round_once_fp16s(pops)
         lat.upload_pops(pops)
         del pops
         lat.step(steps - steps // 2)
         _, u = lat.rhou(key=2, dtype=np.float64)
         lat.close()
         out[model]["fp64_one_fp16s_rounding_rel_l2_u"] = float(np.linalg.norm(u - us["fp64"]) / ref)
+        if beyond:
+            out[model]["fp64_values_beyond_fp16s"] = beyond
         del u
         if model == "les":
             # FP64 runs from initial populations perturbed by eps (relative,
@@ -644,7 +651,8 @@ def run_ours(args, rank, world, local_rank):
             if storage == "fp16s":
                 variants[key]["rounding"] = used
         extras["variants"] = variants
-        acc = accuracy_block(F, args.accuracy_ni, 2000, keep_bgk_fp32=args.accuracy_ni == par_ni,
+        acc = accuracy_block(F, args.accuracy_ni, args.accuracy_steps,
+                             keep_bgk_fp32=args.accuracy_ni == par_ni and args.accuracy_steps == 2000,
                              models=tuple(args.accuracy_models.split(",")))
         extras["accuracy"], kept = acc if isinstance(acc, tuple) else (acc, None)
         extras["blocks_256"] = blocks_block(F, torch, stream, 256, args.steps)
@@ -766,6 +774,8 @@ def main():
                          "the autotuner (profiling)")
     ap.add_argument("--accuracy-ni", type=int, default=256,
                     help="cavity size of the FP64-referenced velocity error report (256 or 512)")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="steps of the velocity error report (the configuration's 2000)")
     ap.add_argument("--accuracy-models", default="bgk,mrt,les",
                     help="models of the velocity error report (comma-separated)")
     ap.add_argument("--no-parity", action="store_true",
@@ -792,7 +802,7 @@ def main():
         if args.only == "blocks":
             out = {"blocks_256": blocks_block(F, torch, stream, 256, args.steps)}
         elif args.only == "accuracy":
-            out = {"accuracy": accuracy_block(F, args.accuracy_ni, 2000,
+            out = {"accuracy": accuracy_block(F, args.accuracy_ni, args.accuracy_steps,
                                               models=tuple(args.accuracy_models.split(",")))}
         else:
             out = {"ensemble_128": ensemble_block(F, torch, stream)}

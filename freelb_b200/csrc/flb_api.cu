@@ -1714,7 +1714,7 @@ int flb_check_finite(flb_lattice* h, uint64_t* bad, void* stream) {
     using R = std::remove_pointer_t<decltype(rp)>;
     return for_blocks(h, [&](const HostBlock& b) {
       k_finite<S, R><<<grid_1d(b.padded()), 256, 0, st>>>(
-          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, acc, h->sp);
+          b.L, static_cast<const S*>(h->pops[h->cur]) + b.base, h->flags + b.base, acc, h->sp);
       return FLB_OK;
     });
   }));

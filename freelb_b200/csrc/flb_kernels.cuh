@@ -324,13 +324,15 @@ static __global__ void __launch_bounds__(256) k_sum_partials(const double* parti
 
 template <typename S, typename R>
 __global__ void __launch_bounds__(256) k_finite(LayoutParams L, const S* pops,
-                                                unsigned long long* acc, StepParams sp) {
+                                                const uint8_t* flags, unsigned long long* acc,
+                                                StepParams sp) {
   unsigned long long bad = 0;
   const long long total = L.plane * L.nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
        c += (long long)gridDim.x * blockDim.x) {
     int x, y, z;
     if (!decode_cell(L, c, x, y, z)) continue;
+    if (select_op(sp, flags[c]) == OP_NONE) continue;  // void: the reference's wrapped values
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
       const R v = Storage<S, R>::load(pops + i * L.dstride + c, sp.shift[i], sp.inv_scale);

@@ -237,7 +237,10 @@ FLB_API int flb_reduce_conservation(flb_lattice* lat, uint8_t key, double out[4]
  * BlockLattice::getToleranceU (block_lattice.hh:266-288). */
 FLB_API int flb_tolerance_u(flb_lattice* lat, uint8_t key, double* max_du, void* stream);
 
-/* Non-finite check of the populations: *bad = number of non-finite values;
+/* Non-finite check of the populations of every cell whose flag selects an
+ * op (void cells, which only carry the reference's wrapped values, are left
+ * out: over long FP16S runs such values can leave the binary16 range without
+ * touching any cell that is updated): *bad = number of non-finite values;
  * returns FLB_ERR_NUMERIC when that number is not zero. */
 FLB_API int flb_check_finite(flb_lattice* lat, uint64_t* bad, void* stream);
 

@@ -167,9 +167,9 @@ def test_conservation_and_tolerance(gpu_ok):
 
 
 def test_non_finite_populations_are_reported(gpu_ok):
-    """flb_check_finite counts non-finite populations and returns
-    FLB_ERR_NUMERIC when there are any (a NaN uploaded on the host; stepping it
-    only spreads the NaN)."""
+    """flb_check_finite counts non-finite populations of the cells the step
+    updates and returns FLB_ERR_NUMERIC when there are any (a NaN uploaded on
+    the host; stepping it only spreads the NaN); void cells are not checked."""
     import ctypes
     from freelb_b200 import _capi as C
     lat = F.cavity(10)
@@ -183,3 +183,9 @@ def test_non_finite_populations_are_reported(gpu_ok):
     assert rc == C.ERR_NUMERIC and v.value == 1
     lat.step(2)
     assert lat.nonfinite() > 1
+    # a void cell carries only the reference's wrapped values: not counted
+    v2 = F.cavity(10)
+    p2 = v2.download_pops()
+    p2[0] = np.inf                        # rest population of cell 0, a void corner
+    v2.upload_pops(p2)
+    assert v2.nonfinite() == 0
